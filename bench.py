@@ -1,0 +1,329 @@
+"""Benchmark of the DIM RK3 time step on B200 (one JSON line on rank 0).
+
+Workload (N=1): the plain FP64 1024^2 DIM field -- a vapour bubble (seeded
+radius in [0.05, 0.15]) in saturated liquid at T0 = 0.95, Re=5, We=10,
+Pr=20, cv_r=2.5 -- advanced by RK3-TVD steps.  A "step" is one full RK3
+time step (3 stages, boundary passes included) of the whole field.  The
+metric is interior cell-updates per second (1 cell-update = one RK3 step of
+one interior cell).  Inputs are seeded synthetic arrays of that shape.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--gpus N > 1 runs under torchrun, one rank per GPU, each rank advancing
+its own field (replicas: the north-star domain is never sharded), so the
+scaling is weak; value = all ranks' cell-updates / max-over-ranks time.
+
+--impl reference times the reference algorithm's CPU restatement (the
+oracle, all host threads) on the same workload, each step a bounded
+sample of rows of that field (the reference's Fortran cannot be built on
+this image: no Fortran compiler, no netCDF).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_INTERIOR = 1024
+BYTES_PER_CELL_UPDATE = 256  # 3 stage writes + 3 stage reads + 2 reads of u^n, 32 B each
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=N_INTERIOR)
+    ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--bc", default="periodic_xy")
+    return ap.parse_args()
+
+
+def workload(n, seed, rank=0):
+    from dim2d_finite_volume_b200 import ic
+    rng = np.random.default_rng(seed + rank)
+    nx, ny, x_map, y_map = ic.grid(n)
+    dx = x_map[1] - x_map[0]
+    r = float(rng.uniform(0.05, 0.15))
+    q = ic.bubbles(x_map, y_map, 0.95, [(0.0, 0.0, r)], li=4.0 * dx)
+    # periodic ghosts as field%ini leaves them
+    px, py = nx - 4, ny - 4
+    q[:, :, 0:2] = q[:, :, px:px + 2]
+    q[:, :, nx - 2:] = q[:, :, 2:4]
+    q[:, 0:2, :] = q[:, py:py + 2, :]
+    q[:, ny - 2:, :] = q[:, 2:4, :]
+    rho_min = float(q[0].min())
+    dt = min(ic.cfl_dt(q, dx, dx, 0.1), 0.2 * 5.0 * rho_min * dx * dx)
+    return dict(nx=nx, ny=ny, x_map=x_map, y_map=y_map, nodes=np.ascontiguousarray(q), dt=dt,
+                radius=r)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per launch of the interior stage kernel from the committed
+    ncu summary (profiles/interior_stage_traffic.json), per interior cell."""
+    p = os.path.join(ROOT, "profiles", "interior_stage_traffic.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("dram_bytes_per_cell_per_launch")
+    return None
+
+
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+            self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % os.getpid())
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(w, budget_s=15.0, threads=None):
+    """Oracle (CPU restatement) on a bounded sample: full RK3 steps of a
+    row band of the same field, repeated until budget_s of host time."""
+    from oracle import oracle as O
+    nth = threads or os.cpu_count() or 1
+    O.set_threads(nth)
+    nx = w["nx"]
+    band = 64 + 4  # 64 interior rows + ghosts, periodic in y
+    q = np.ascontiguousarray(w["nodes"][:, :band, :])
+    y_map = w["y_map"][:band]
+    cfg = O.make_cfg(nx, band, periodic=True)
+    O.apply_bc_on_nodes(cfg, 0.0, w["x_map"], y_map, q.copy(), q)
+    cells = (nx - 4) * (band - 4)
+    steps, t0 = 0, time.perf_counter()
+    t = 0.0
+    while True:
+        t = O.integrate(cfg, q, w["x_map"], y_map, t, w["dt"], 1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s:
+            break
+    return {"value": cells * steps / el, "unit": "cell-updates/s", "cores": nth, "kind": "port",
+            "sample": "%d RK3 steps of a %dx%d periodic band (interior %dx%d) of the %d^2 "
+                      "field, %.1f s" % (steps, nx, band, nx - 4, band - 4, nx - 4, el)}
+
+
+def run_reference(a, rank, world):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    w = workload(a.n, a.seed)
+    nth = os.cpu_count() or 1
+    O.set_threads(nth)
+    nx = w["nx"]
+    band = 32 + 4
+    q = np.ascontiguousarray(w["nodes"][:, :band, :])
+    y_map = w["y_map"][:band]
+    cfg = O.make_cfg(nx, band, periodic=True)
+    O.apply_bc_on_nodes(cfg, 0.0, w["x_map"], y_map, q.copy(), q)
+    cells = (nx - 4) * (band - 4)
+    t = 0.0
+    for _ in range(a.warmup):
+        t = O.integrate(cfg, q, w["x_map"], y_map, t, w["dt"], 1)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        t = O.integrate(cfg, q, w["x_map"], y_map, t, w["dt"], 1)
+    el = time.perf_counter() - t0
+    v = cells * a.steps / el
+    line = {
+        "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * el / a.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": "plain FP64 DIM %d^2 field, RK3 step, row-band sample" % a.n,
+                   "sample_rows": band - 4, "bc": "periodic_xy"},
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": nth, "kind": "port",
+                         "sample": "each step: one RK3 step of a %dx%d band of the %d^2 field"
+                                   % (nx, band, a.n)},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        return run_reference(a, rank, world)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    from dim2d_finite_volume_b200 import field as F
+
+    w = workload(a.n, a.seed, rank)
+    nx, ny = w["nx"], w["ny"]
+    cells = (nx - 4) * (ny - 4)
+    dt = w["dt"]
+    stream = torch.cuda.Stream()
+    fld = F.Field(nx, ny, bc=a.bc)
+    fld.set_stream(stream.cuda_stream)
+    fld.ini(w["nodes"], w["x_map"], w["y_map"])
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident timing (value) --------------------------------
+    for _ in range(max(3, a.warmup)):
+        fld.integrate(dt, 1)
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(a.steps)]
+    n_launch0 = fld.launches
+    fld.profile(True)
+    barrier()
+    with torch.cuda.stream(stream):
+        for k in range(a.steps):
+            flush.fill_(float(k))  # L2 flush between timed steps (outside the events)
+            ev[k][0].record(stream)
+            fld.integrate(dt, 1)
+            ev[k][1].record(stream)
+    barrier()
+    prof_ms, prof_n = fld.profile_read()
+    fld.profile(False)
+    launches = fld.launches - n_launch0
+    step_ms = sum(s.elapsed_time(e) for s, e in ev)
+    # ---- end-to-end through the public API with host buffers ----------
+    host_in = torch.empty((4, ny, nx), dtype=torch.float64, pin_memory=True)
+    host_in.copy_(torch.from_numpy(w["nodes"]))
+    host_out = torch.empty((4, ny, nx), dtype=torch.float64, pin_memory=True)
+    hin = host_in.numpy()
+    hout = host_out.numpy()
+    e2e_steps = max(3, a.steps // 2)
+    for _ in range(2):
+        fld.ini(hin, w["x_map"], w["y_map"])
+        fld.integrate(dt, 1)
+        fld.download(hout)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        fld.ini(hin, w["x_map"], w["y_map"])  # H2D of the step's input nodes
+        fld.integrate(dt, 1)
+        fld.download(hout)                    # D2H of the step's result nodes
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    fld.close()
+
+    t = torch.tensor([step_ms, e2e_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms, e2e_ms = float(t[0]), float(t[1])
+    total_cells = cells * world
+    value = total_cells * a.steps / (step_ms * 1e-3)
+    e2e_value = total_cells * e2e_steps / (e2e_ms * 1e-3)
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        per_launch_ms = prof_ms / max(1, prof_n)
+        bytes_per_launch = cells * BYTES_PER_CELL_UPDATE / 3.0
+        achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+        tr = profile_traffic()
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+            "n_gpus": world, "steps": a.steps, "warmup": max(3, a.warmup),
+            "ms_per_step": step_ms / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "plain FP64 DIM %d^2 (+2 ghosts) bubble, T0=0.95, RK3 step"
+                                   % a.n, "bc": a.bc, "nx": nx, "ny": ny, "dt": dt,
+                       "l2": "flushed between timed steps (2x L2 write, outside the events)",
+                       "replicas_per_gpu": 1},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "kernel": "k_interior<1> (fused RK3 stage)",
+                         "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "launch_ms": per_launch_ms,
+                         "traffic": (tr * cells if tr is not None else None)},
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": int(hin.nbytes + w["x_map"].nbytes + w["y_map"].nbytes),
+                    "d2h_bytes_per_step": int(hout.nbytes),
+                    "note": "each step: dim2d_upload (pinned host nodes) + dim2d_step(1) + "
+                            "dim2d_download"},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        line["cpu_baseline"] = cpu_baseline(w)
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

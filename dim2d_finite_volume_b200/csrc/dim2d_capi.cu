@@ -1,0 +1,355 @@
+// dim2d_capi.cu -- the extern "C" boundary (include/dim2d.h) over the
+// sm_100a kernels.  One handle owns one field resident in HBM: three
+// pitched FP64 copies (u^n, and the two stage buffers the RK3 scheme
+// ping-pongs through) plus x_map / y_map.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/dim2d.h"
+#include "dim2d_kernels.cuh"
+#include "dim2d_internal.h"
+
+using namespace dim2d;
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+namespace dim2d {
+
+int set_error(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_error(cudaError_t e, const char* where) {
+  return set_error(DIM2D_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+DimConst make_const(const dim2d_params& p) {
+  DimConst k{};
+  k.re = p.re;
+  k.we = p.we;
+  k.pr = p.pr;
+  k.cv_r = p.cv_r;
+  k.viscous_r = p.viscous_r;
+  k.ire = 1.0 / p.re;
+  k.iwe = 1.0 / p.we;
+  k.ipr = 1.0 / p.pr;
+  k.irepr = 1.0 / (p.re * p.pr);
+  k.c15cv = 1.5 / p.cv_r;
+  k.c3cv = 3.0 / p.cv_r;
+  k.two_mu = 2.0 + p.viscous_r;
+  k.gravity_ac = p.gravity_ac;
+  k.gravity = p.gravity;
+  return k;
+}
+
+int pitch_for(int nx) { return (nx + 15) / 16 * 16; }
+
+// Resolve the reference's per-section bc choices into per-side kinds
+// (library_config.py:41-230 maps the presets onto these choices).
+int resolve_sides(const int bc_choice[8], const int bc_type[8], int side_kind[8], int* periodic) {
+  int nper = 0;
+  for (int s = 0; s < 8; s++) {
+    const int c = bc_choice[s];
+    if (c == DIM2D_PERIODIC_X || c == DIM2D_PERIODIC_Y) {
+      side_kind[s] = SIDE_PERIODIC;
+      nper++;
+    } else if (c == DIM2D_WALL) {
+      side_kind[s] = SIDE_WALL;
+    } else if (c == DIM2D_HEDSTROM) {
+      side_kind[s] = SIDE_OPEN;
+    } else if (c == DIM2D_REFLECTION_X || c == DIM2D_REFLECTION_Y) {
+      side_kind[s] = SIDE_REFLECT;
+    } else {
+      return set_error(DIM2D_ERR_ARG, "bc_choice[%d] = %d is not a known choice", s, c);
+    }
+    if (bc_type[s] < 0 || bc_type[s] > 3)
+      return set_error(DIM2D_ERR_ARG, "bc_type[%d] = %d is not a known type", s, bc_type[s]);
+  }
+  if (nper != 0 && nper != 8)
+    return set_error(DIM2D_ERR_UNSUPPORTED,
+                     "periodic boundaries must be periodic on all sides (periodic_xy)");
+  *periodic = nper == 8;
+  return DIM2D_OK;
+}
+
+}  // namespace dim2d
+
+extern "C" {
+
+void dim2d_default_params(dim2d_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof *p);
+  p->re = 5.0;
+  p->we = 10.0;
+  p->pr = 20.0;
+  p->cv_r = 2.5;
+  p->viscous_r = -1.5;
+  p->gravity_ac = 0;
+  p->gravity = 0.0;
+  p->wall_micro_contact_angle = 90.0;
+  p->wall_heat_source_choice = 0;
+  p->wall_maximum_heat_flux = 0.0;
+  p->wall_heat_source_center = 0.0;
+  p->wall_heat_source_variance = 1.0;
+  p->obc_eigenqties_strategy = 0;
+  p->obc_edge_flux_strategy = 0;
+  p->T0 = 0.95;
+  p->flow_velocity = 0.0;
+}
+
+const char* dim2d_last_error(void) { return g_last_error.c_str(); }
+const char* dim2d_version(void) { return "dim2d-b200 0.1 (sm_100a)"; }
+
+int dim2d_ini_coordinates(int nx, int ny, double x_min, double x_max, double y_min, double y_max,
+                          double* x_map, double* y_map) {
+  if (nx < 2 * BC + 2 || ny < 2 * BC + 2 || !x_map || !y_map)
+    return set_error(DIM2D_ERR_ARG, "ini_coordinates: bad arguments");
+  const double dx = (x_max - x_min) / (nx - 1 - 2 * BC);
+  const double dy = (y_max - y_min) / (ny - 1 - 2 * BC);
+  for (int i = 1; i <= nx; i++) x_map[i - 1] = x_min + (i - 1 - BC) * dx;
+  for (int j = 1; j <= ny; j++) y_map[j - 1] = y_min + (j - 1 - BC) * dy;
+  return DIM2D_OK;
+}
+
+int dim2d_create(const dim2d_params* p, int nx, int ny, const int bc_choice[8],
+                 const int bc_type[8], const int bc_order[8], int precision,
+                 dim2d_handle** out) {
+  if (!p || !bc_choice || !bc_type || !bc_order || !out)
+    return set_error(DIM2D_ERR_ARG, "create: null argument");
+  *out = nullptr;
+  if (nx < 8 || ny < 8)
+    return set_error(DIM2D_ERR_ARG, "create: nx, ny must be >= 8 (got %d x %d)", nx, ny);
+  if (nx > 65536 || ny > 65536)
+    return set_error(DIM2D_ERR_ARG, "create: nx, ny must be <= 65536");
+  if (precision != DIM2D_FP64 && precision != DIM2D_MIXED)
+    return set_error(DIM2D_ERR_ARG, "create: unknown precision %d", precision);
+  if (!(p->re > 0) || !(p->we > 0) || !(p->pr > 0) || !(p->cv_r > 0))
+    return set_error(DIM2D_ERR_ARG, "create: re, we, pr, cv_r must be positive");
+  int side_kind[8], periodic = 0;
+  int rc = resolve_sides(bc_choice, bc_type, side_kind, &periodic);
+  if (rc) return rc;
+  if (!periodic)
+    return set_error(DIM2D_ERR_UNSUPPORTED,
+                     "create: only the periodic_xy configuration is provided by this build");
+  if (precision != DIM2D_FP64)
+    return set_error(DIM2D_ERR_UNSUPPORTED, "create: mixed precision not provided by this build");
+
+  dim2d_handle* h = new dim2d_handle();
+  h->p = *p;
+  h->k = make_const(*p);
+  h->precision = precision;
+  h->periodic = periodic;
+  std::memcpy(h->bc_choice, bc_choice, sizeof h->bc_choice);
+  std::memcpy(h->bc_type, bc_type, sizeof h->bc_type);
+  std::memcpy(h->bc_order, bc_order, sizeof h->bc_order);
+  std::memcpy(h->side_kind, side_kind, sizeof h->side_kind);
+  h->f.nx = nx;
+  h->f.ny = ny;
+  h->f.pitch = pitch_for(nx);
+  h->f.plane = (size_t)ny * h->f.pitch;
+  cudaError_t e = cudaGetDevice(&h->device);
+  if (e != cudaSuccess) {
+    delete h;
+    return cuda_error(e, "create: cudaGetDevice");
+  }
+  const size_t bytes = 4 * h->f.plane * sizeof(double);
+  double** bufs[3] = {&h->A, &h->B, &h->C};
+  for (double** b : bufs) {
+    e = cudaMalloc(b, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      dim2d_destroy(h);
+      return set_error(DIM2D_ERR_NOMEM, "create: cudaMalloc of %zu bytes failed: %s", bytes,
+                       cudaGetErrorString(e));
+    }
+  }
+  e = cudaMalloc(&h->x_map, nx * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&h->y_map, ny * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&h->scalar, 4 * sizeof(double));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    dim2d_destroy(h);
+    return set_error(DIM2D_ERR_NOMEM, "create: allocation failed: %s", cudaGetErrorString(e));
+  }
+  h->stream = h->own_stream;
+  // keep never-written pitch padding and ghost cells defined
+  for (double* b : {h->A, h->B, h->C}) cudaMemsetAsync(b, 0, bytes, h->stream);
+  *out = h;
+  return DIM2D_OK;
+}
+
+int dim2d_destroy(dim2d_handle* h) {
+  if (!h) return DIM2D_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  for (cudaEvent_t ev : h->prof_ev) cudaEventDestroy(ev);
+  cudaFree(h->A);
+  cudaFree(h->B);
+  cudaFree(h->C);
+  cudaFree(h->x_map);
+  cudaFree(h->y_map);
+  cudaFree(h->scalar);
+  cudaFree(h->td);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+  return DIM2D_OK;
+}
+
+int dim2d_set_stream(dim2d_handle* h, void* stream) {
+  if (!h) return set_error(DIM2D_ERR_ARG, "set_stream: null handle");
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return DIM2D_OK;
+}
+
+int dim2d_sync(dim2d_handle* h) {
+  if (!h) return set_error(DIM2D_ERR_ARG, "sync: null handle");
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_error(e, "sync");
+  return DIM2D_OK;
+}
+
+int dim2d_upload(dim2d_handle* h, const double* nodes, const double* x_map, const double* y_map,
+                 double t) {
+  if (!h || !nodes || !x_map || !y_map) return set_error(DIM2D_ERR_ARG, "upload: null argument");
+  const Field& f = h->f;
+  cudaError_t e = cudaMemcpy2DAsync(h->A, f.pitch * sizeof(double), nodes, f.nx * sizeof(double),
+                                    f.nx * sizeof(double), 4 * (size_t)f.ny,
+                                    cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h->x_map, x_map, f.nx * sizeof(double), cudaMemcpyHostToDevice,
+                        h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h->y_map, y_map, f.ny * sizeof(double), cudaMemcpyHostToDevice,
+                        h->stream);
+  if (e != cudaSuccess) return cuda_error(e, "upload");
+  // td_operators_class.f:157-158
+  h->dx = x_map[1] - x_map[0];
+  h->dy = y_map[1] - y_map[0];
+  if (!(h->dx > 0) || !(h->dy > 0)) return set_error(DIM2D_ERR_ARG, "upload: x_map/y_map not increasing");
+  h->rdx = 1.0 / h->dx;
+  h->rdy = 1.0 / h->dy;
+  h->x_min = x_map[BC];
+  h->x_max = x_map[f.nx - 1 - BC];
+  h->y_min = y_map[BC];
+  h->y_max = y_map[f.ny - 1 - BC];
+  h->t = t;
+  h->uploaded = true;
+  h->graph_dt = -1.0;  // invalidate captured step graphs
+  return DIM2D_OK;
+}
+
+int dim2d_download(dim2d_handle* h, double* nodes, double* t) {
+  if (!h || !nodes) return set_error(DIM2D_ERR_ARG, "download: null argument");
+  if (!h->uploaded) return set_error(DIM2D_ERR_NOT_READY, "download: no state uploaded");
+  const Field& f = h->f;
+  cudaError_t e = cudaMemcpy2DAsync(nodes, f.nx * sizeof(double), h->A, f.pitch * sizeof(double),
+                                    f.nx * sizeof(double), 4 * (size_t)f.ny,
+                                    cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_error(e, "download");
+  if (t) *t = h->t;
+  return check_status(h);
+}
+
+int dim2d_device_state(dim2d_handle* h, double** nodes, int* pitch) {
+  if (!h) return set_error(DIM2D_ERR_ARG, "device_state: null handle");
+  if (nodes) *nodes = h->A;
+  if (pitch) *pitch = h->f.pitch;
+  return DIM2D_OK;
+}
+
+long long dim2d_launch_count(const dim2d_handle* h) { return h ? h->launches : 0; }
+
+int dim2d_profile(dim2d_handle* h, int enable) {
+  if (!h) return set_error(DIM2D_ERR_ARG, "profile: null handle");
+  h->prof = enable != 0;
+  h->prof_used = 0;
+  return DIM2D_OK;
+}
+
+int dim2d_profile_read(dim2d_handle* h, double* ms, long long* launches) {
+  if (!h || !ms || !launches) return set_error(DIM2D_ERR_ARG, "profile_read: null argument");
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_error(e, "profile_read");
+  double tot = 0.0;
+  for (size_t i = 0; i + 1 < h->prof_used; i += 2) {
+    float m = 0.f;
+    e = cudaEventElapsedTime(&m, h->prof_ev[i], h->prof_ev[i + 1]);
+    if (e != cudaSuccess) return cuda_error(e, "profile_read elapsed");
+    tot += m;
+  }
+  *ms = tot;
+  *launches = (long long)(h->prof_used / 2);
+  return DIM2D_OK;
+}
+
+int dim2d_apply_bc_on_nodes(dim2d_handle* h) {
+  if (!h) return set_error(DIM2D_ERR_ARG, "apply_bc_on_nodes: null handle");
+  if (!h->uploaded) return set_error(DIM2D_ERR_NOT_READY, "apply_bc_on_nodes: no state");
+  return apply_bc_on_nodes(h, h->A, h->A);
+}
+
+int dim2d_time_dev(dim2d_handle* h, double* time_dev) {
+  if (!h || !time_dev) return set_error(DIM2D_ERR_ARG, "time_dev: null argument");
+  if (!h->uploaded) return set_error(DIM2D_ERR_NOT_READY, "time_dev: no state");
+  const Field& f = h->f;
+  cudaError_t e = cudaSuccess;
+  if (!h->td) e = cudaMalloc(&h->td, 4 * f.plane * sizeof(double));
+  if (e != cudaSuccess) return set_error(DIM2D_ERR_NOMEM, "time_dev: %s", cudaGetErrorString(e));
+  // td_operators_class.f:150-154: every cell starts at debug_real
+  e = launch_fill(h->td, 9.9692099683868690e+36, 4 * f.plane, h->stream);
+  h->launches++;
+  if (e == cudaSuccess) {
+    e = launch_time_dev(h->A, h->td, f, h->rdx, h->rdy, h->k, h->stream);
+    h->launches++;
+  }
+  if (e != cudaSuccess) return cuda_error(e, "time_dev");
+  e = cudaMemcpy2DAsync(time_dev, f.nx * sizeof(double), h->td, f.pitch * sizeof(double),
+                        f.nx * sizeof(double), 4 * (size_t)f.ny, cudaMemcpyDeviceToHost,
+                        h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_error(e, "time_dev copy");
+  return DIM2D_OK;
+}
+
+int dim2d_cfl_dt(dim2d_handle* h, double cfl, double* dt) {
+  if (!h || !dt || !(cfl > 0)) return set_error(DIM2D_ERR_ARG, "cfl_dt: bad argument");
+  if (!h->uploaded) return set_error(DIM2D_ERR_NOT_READY, "cfl_dt: no state");
+  cudaError_t e = launch_cfl_max(h->A, h->f, h->k, h->scalar, h->stream);
+  h->launches++;
+  double smax = 0.0;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&smax, h->scalar, sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_error(e, "cfl_dt");
+  if (!(smax > 0) || !std::isfinite(smax))
+    return set_error(DIM2D_ERR_ARG, "cfl_dt: max(c+|u|) = %g is not a positive finite value", smax);
+  *dt = cfl * std::fmin(h->dx, h->dy) / smax;
+  return DIM2D_OK;
+}
+
+int dim2d_step(dim2d_handle* h, double dt, int nsteps) {
+  if (!h) return set_error(DIM2D_ERR_ARG, "step: null handle");
+  if (!h->uploaded) return set_error(DIM2D_ERR_NOT_READY, "step: no state uploaded");
+  if (nsteps < 0 || !std::isfinite(dt)) return set_error(DIM2D_ERR_ARG, "step: bad dt/nsteps");
+  for (int s = 0; s < nsteps; s++) {
+    int rc = rk3_step(h, dt);
+    if (rc) return rc;
+  }
+  return DIM2D_OK;
+}
+
+}  // extern "C"

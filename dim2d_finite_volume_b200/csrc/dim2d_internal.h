@@ -1,0 +1,58 @@
+// dim2d_internal.h -- host-side handle and helpers behind include/dim2d.h.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <vector>
+
+#include "../../include/dim2d.h"
+#include "dim2d_kernels.cuh"
+
+struct dim2d_handle {
+  int device = 0;
+  dim2d_params p{};
+  dim2d::DimConst k{};
+  int precision = 0;
+  int periodic = 0;
+  int bc_choice[8]{}, bc_type[8]{}, bc_order[8]{};
+  int side_kind[8]{};
+  dim2d::Field f{};
+  // A = u^n (the field), B and C = stage buffers
+  double* A = nullptr;
+  double* B = nullptr;
+  double* C = nullptr;
+  double* td = nullptr;  // time_dev buffer, allocated on first use
+  double* x_map = nullptr;
+  double* y_map = nullptr;
+  double* scalar = nullptr;  // reductions / status words
+  double dx = 0, dy = 0, rdx = 0, rdy = 0;
+  double x_min = 0, x_max = 0, y_min = 0, y_max = 0;
+  double t = 0;
+  bool uploaded = false;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  long long launches = 0;
+  // captured two-step graph (A -> B -> A), valid for graph_dt
+  cudaGraphExec_t graph_exec = nullptr;
+  double graph_dt = -1.0;
+  // live timing of the interior stage kernel (dim2d_profile)
+  bool prof = false;
+  std::vector<cudaEvent_t> prof_ev;  // start/stop pairs
+  size_t prof_used = 0;
+};
+
+namespace dim2d {
+int set_error(int code, const char* fmt, ...);
+int cuda_error(cudaError_t e, const char* where);
+DimConst make_const(const dim2d_params& p);
+int pitch_for(int nx);
+int resolve_sides(const int bc_choice[8], const int bc_type[8], int side_kind[8], int* periodic);
+}  // namespace dim2d
+
+// dim2d_step.cu
+int rk3_step(dim2d_handle* h, double dt);
+int apply_bc_on_nodes(dim2d_handle* h, const double* nodes_tmp, double* nodes);
+int check_status(dim2d_handle* h);
+// bracket one launch with profiling events (no-op unless h->prof)
+void prof_begin(dim2d_handle* h);
+void prof_end(dim2d_handle* h);

@@ -1,0 +1,144 @@
+// dim2d_physics.cuh -- DIM (van der Waals + Korteweg) physics for the
+// sm_100a kernels: per-node primitives and the face flux in a frame
+// (n = face normal, t = tangential) so one routine serves x- and y-faces.
+//
+// Reference formulas (paths relative to the reference project root):
+//   primitives   src/physical_models/dim2d/dim2d_prim_module.f:242-289,
+//                392-453 (pressure), 515-613 (temperatures), 1056-1155
+//   face fluxes  src/physical_models/dim2d/dim2d_fluxes_module.f:103-1649
+//   operators    src/sd_operators/mattsson_operators/sd_operators_class.f
+//                :160-1039 and sd_operators_fd_module.f:71-153
+//
+// Evaluation differs from the reference only by rounding: primitives are
+// computed once per node instead of once per operator call, products such
+// as rho*u*u use the node velocity, and divisions by dx use 1/dx.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace dim2d {
+
+// Physical constants (dim2d_parameters.f:146-199) and their derived
+// coefficients, computed once on the host.
+struct DimConst {
+  double re, we, pr, cv_r, viscous_r;
+  double ire;        // 1/Re        (dim2d_fluxes_module.f:210)
+  double iwe;        // 1/We        (dim2d_fluxes_module.f:212)
+  double ipr;        // 1/Pr        (dim2d_fluxes_module.f:1285)
+  double irepr;      // 1/(Re*Pr)   (dim2d_fluxes_module.f:1385)
+  double c15cv;      // 1.5/cv_r    (dim2d_fluxes_module.f:691)
+  double c3cv;       // 3/cv_r      (dim2d_prim_module.f:433)
+  double two_mu;     // 2+viscous_r (dim2d_fluxes_module.f:636)
+  int gravity_ac;
+  double gravity;
+};
+
+// Per-node primitive quantities used by the flux formulas.
+struct NodePrim {
+  double u, v;   // velocity_x/y           (prim :242-289)
+  double p;      // classical_pressure     (prim :425-453)
+  double tcl;    // classical_temperature_eff (prim :515-544)
+  double cp;     // capillarity_pressure 1/(3-rho) (prim :1056-1071)
+};
+
+__host__ __device__ __forceinline__ NodePrim node_prim(double r, double mx, double my, double e,
+                                                       const DimConst& k) {
+  NodePrim o;
+  const double ir = 1.0 / r;
+  o.u = mx * ir;
+  o.v = my * ir;
+  o.cp = 1.0 / (3.0 - r);
+  // W = E - rho|u|^2/2 + 3 rho^2 ; P = 3/((3-rho) cv_r) W - 3 rho^2 ; Tcl = W/rho
+  const double w = e - 0.5 * r * (o.u * o.u + o.v * o.v) + 3.0 * (r * r);
+  o.p = k.c3cv * o.cp * w - 3.0 * (r * r);
+  o.tcl = ir * w;
+  return o;
+}
+
+// capillarity_temperature_eff with centred gradients (prim :582-613,
+// sd_operators_fd_module.f:71-153): 0.5/rho * (drho/dx^2 + drho/dy^2).
+__host__ __device__ __forceinline__ double node_tcap(double r, double rxm, double rxp, double rym,
+                                                     double ryp, double hrdx, double hrdy) {
+  const double gx = hrdx * (rxp - rxm);
+  const double gy = hrdy * (ryp - rym);
+  return 0.5 / r * (gx * gx + gy * gy);
+}
+
+// Inputs of one face flux, in the face frame.  "a" is the node on the low
+// side of the face, "b" the node on the high side.
+struct FaceIn {
+  // conservative values: rho, momentum along n, momentum along t, energy
+  double ra, rb, mna, mnb, mta, mtb, ea, eb;
+  // primitives: velocity along n / t, pressure, Tcl, cp, Tcap
+  double una, unb, uta, utb, pa, pb, ta, tb, ca, cb, ka, kb;
+  // derivatives at the face
+  double drn, drt;  // d rho / dn, d rho / dt
+  double dunn;      // d u_n / dn
+  double dunt;      // d u_n / dt
+  double dutn;      // d u_t / dn
+  double dutt;      // d u_t / dt
+  double lap;       // d2 rho/dn2 + d2 rho/dt2
+  double dtn;       // d Tcl / dn
+  double dkn;       // d Tcap / dn
+};
+
+// Face flux of the 4 conservative variables; out = {mass, momentum_n,
+// momentum_t, energy}.  For an x-face n = x (dim2d_fluxes_module.f:103-117,
+// 193-222, 319-348, 445-477 and the parts they call); for a y-face n = y
+// (:145-159, 256-285, 382-411, 511-541), momentum_n is then momentum_y.
+__host__ __device__ __forceinline__ void face_flux(const FaceIn& f, const DimConst& k,
+                                                   double out[4]) {
+  const double avr = 0.5 * (f.ra + f.rb);
+  const double avmn = 0.5 * (f.mna + f.mnb);
+  const double avun = 0.5 * (f.una + f.unb);
+  const double avut = 0.5 * (f.uta + f.utb);
+  const double drn2 = f.drn * f.drn;
+  const double drt2 = f.drt * f.drt;
+  const double grad2 = drn2 + drt2;
+
+  // mass: f(momentum_n)
+  out[0] = avmn;
+
+  // normal momentum: inviscid f(m_n u_n) + f(P); viscid (2+mu) du_n/dn +
+  // mu du_t/dt; capillarity 1.5/cv f(cp) |grad rho|^2 + f(rho) lap rho
+  // + 0.5 (drho_t^2 - drho_n^2)
+  {
+    const double inv = 0.5 * (f.mna * f.una + f.mnb * f.unb) + 0.5 * (f.pa + f.pb);
+    const double vis = k.two_mu * f.dunn + k.viscous_r * f.dutt;
+    const double cap = k.c15cv * (0.5 * (f.ca + f.cb)) * grad2 + avr * f.lap +
+                       0.5 * (-drn2 + drt2);
+    out[1] = inv - k.ire * vis - k.iwe * cap;
+  }
+  // tangential momentum: inviscid f(m_t u_n); viscid du_n/dt + du_t/dn;
+  // capillarity -drho_n drho_t
+  {
+    const double inv = 0.5 * (f.mta * f.una + f.mtb * f.unb);
+    const double vis = f.dunt + f.dutn;
+    const double cap = -f.drn * f.drt;
+    out[2] = inv - k.ire * vis - k.iwe * cap;
+  }
+  // energy
+  {
+    const double inv = 0.5 * (f.ea * f.una + f.eb * f.unb) + 0.5 * (f.pa * f.una + f.pb * f.unb);
+    const double vis = avun * (k.two_mu * f.dunn + k.viscous_r * f.dutt) +
+                       avut * (f.dunt + f.dutn) + k.ipr * f.dtn;
+    const double cap = k.c15cv * (0.5 * (f.ca * f.una + f.cb * f.unb)) * grad2 + avmn * f.lap +
+                       0.5 * avun * (-drn2 + drt2) - f.drn * f.drt * avut -
+                       avr * f.drn * (f.dunn + f.dutt) - k.irepr * f.dkn;
+    out[3] = inv - k.ire * vis - k.iwe * cap;
+  }
+}
+
+// Speed of sound, dim2d_prim_module.f:1179-1215.
+__host__ __device__ __forceinline__ double sound_speed(double r, double mx, double my, double e,
+                                                       const DimConst& k) {
+  const double u = mx / r, v = my / r;
+  const double p = 3.0 / ((3.0 - r) * k.cv_r) * (e - 0.5 * r * (u * u + v * v) + 3.0 * (r * r)) -
+                   3.0 * (r * r);
+  const double ee = p + (r * r) * (-3.0 + 2.0 * r);
+  const double b = sqrt((p + 3.0 * (r * r)) / (k.cv_r * ee));
+  const double a = 1.0 / sqrt(1.0 + b * b);
+  const double d = sqrt(r * r * r) * sqrt((3.0 - r) / ee);
+  return sqrt(3.0) * r / (a * d);
+}
+
+}  // namespace dim2d

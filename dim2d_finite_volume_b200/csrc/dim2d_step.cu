@@ -1,0 +1,85 @@
+// dim2d_step.cu -- one RK3-TVD time step on the device
+// (td_integrator_class.f:103-161 with rk3tvd_steps_module.f:52-490).
+//
+// Buffers: A holds u^n.  Stage 1 writes B = A + dt L(A); stage 2 writes
+// C = 3/4 A + 1/4 (B + dt L(B)); stage 3 writes B = 1/3 A + 2/3 (C + dt L(C));
+// then A and B swap.  u^n stays intact in A until the last boundary pass,
+// which the wall operator reads as nodes_tmp (bc_operators_wall_xy_class.f).
+// Each stage is followed by the node boundary pass; for periodic fields the
+// stage kernel writes the ghost images itself.
+#include <utility>
+
+#include "dim2d_internal.h"
+
+using namespace dim2d;
+
+int apply_bc_on_nodes(dim2d_handle* h, const double* nodes_tmp, double* nodes) {
+  (void)nodes_tmp;
+  if (h->periodic) {
+    cudaError_t e = launch_periodic_ghosts(nodes, h->f, h->stream);
+    h->launches++;
+    if (e != cudaSuccess) return cuda_error(e, "apply_bc_on_nodes(periodic)");
+    return DIM2D_OK;
+  }
+  return set_error(DIM2D_ERR_UNSUPPORTED, "apply_bc_on_nodes: configuration not provided");
+}
+
+void prof_begin(dim2d_handle* h) {
+  if (!h->prof) return;
+  if (h->prof_used + 2 > h->prof_ev.size()) {
+    for (int i = 0; i < 64; i++) {
+      cudaEvent_t ev;
+      if (cudaEventCreate(&ev) != cudaSuccess) {
+        h->prof = false;
+        return;
+      }
+      h->prof_ev.push_back(ev);
+    }
+  }
+  cudaEventRecord(h->prof_ev[h->prof_used], h->stream);
+}
+
+void prof_end(dim2d_handle* h) {
+  if (!h->prof) return;
+  cudaEventRecord(h->prof_ev[h->prof_used + 1], h->stream);
+  h->prof_used += 2;
+}
+
+int check_status(dim2d_handle* h) {
+  (void)h;
+  return DIM2D_OK;
+}
+
+static int stage(dim2d_handle* h, int st, const double* uin, double* uout, double dt) {
+  StageArgs a{};
+  a.uin = uin;
+  a.u0 = h->A;
+  a.uout = uout;
+  a.f = h->f;
+  a.dx = h->dx;
+  a.dy = h->dy;
+  a.rdx = h->rdx;
+  a.rdy = h->rdy;
+  a.dt = dt;
+  a.stage = st;
+  a.b = st == 2 ? 0.75 : (st == 3 ? 1.0 / 3.0 : 0.0);  // rk3tvd_steps_module.f:225,444
+  a.periodic = h->periodic;
+  a.k = h->k;
+  prof_begin(h);
+  cudaError_t e = launch_interior_stage(a, h->stream);
+  prof_end(h);
+  h->launches++;
+  if (e != cudaSuccess) return cuda_error(e, "rk3 stage");
+  if (!h->periodic) return apply_bc_on_nodes(h, h->A, uout);
+  return DIM2D_OK;
+}
+
+int rk3_step(dim2d_handle* h, double dt) {
+  int rc = stage(h, 1, h->A, h->B, dt);
+  if (!rc) rc = stage(h, 2, h->B, h->C, dt);
+  if (!rc) rc = stage(h, 3, h->C, h->B, dt);
+  if (rc) return rc;
+  std::swap(h->A, h->B);
+  h->t += dt;  // field_class.f:70
+  return DIM2D_OK;
+}

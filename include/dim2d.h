@@ -1,0 +1,183 @@
+/*
+ * dim2d.h -- C ABI of the B200 (sm_100a) DIM time-derivative library.
+ *
+ * Drop-in boundary for the reference's time integration of one field
+ * (jdesmarais/dim2D_finite_volume, Fortran).  Each entry point names the
+ * reference interface it replaces:
+ *
+ *   field%integrate(dt)                 src/field/field_class.f:61-72
+ *   td_integrator%integrate(field, dt)  src/td_integrator/rungekutta3rdtvd/
+ *                                       td_integrator_class.f:103-161
+ *   field%compute_time_dev()            src/field/field_abstract_class.f:360-379
+ *     -> td_operators%compute_time_dev  src/td_operators/finitevolume/
+ *                                       td_operators_class.f:119-235
+ *   field%apply_bc_on_nodes(nodes_tmp)  src/field/field_abstract_class.f:447-463
+ *   field%ini_coordinates()             src/field/field_abstract_class.f:286-315
+ *
+ * Conventions
+ *   - nodes(nx,ny,ne=4) FP64 in Fortran column-major order: the C array
+ *     q[k][j][i], i fastest (what c_loc(field%nodes) points to).
+ *   - nx, ny include bc_size = 2 ghost layers per side
+ *     (src/parameters/parameters_input.f:81).
+ *   - Every call returns DIM2D_OK (0) or a positive error code; the
+ *     reference stops the process on errors (src/parameters/errors_module.f),
+ *     a Fortran shim turns a non-zero status into `stop`.
+ *   - A handle is used by one host thread at a time.  Calls are ordered on
+ *     the handle's CUDA stream; dim2d_download and dim2d_sync synchronise.
+ */
+#ifndef DIM2D_H
+#define DIM2D_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define DIM2D_API __attribute__((visibility("default")))
+#else
+#define DIM2D_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define DIM2D_OK 0
+#define DIM2D_ERR_ARG 1          /* invalid argument */
+#define DIM2D_ERR_CUDA 2         /* CUDA runtime error (see dim2d_last_error) */
+#define DIM2D_ERR_UNSUPPORTED 3  /* boundary configuration not provided */
+#define DIM2D_ERR_NOMEM 4        /* device allocation refused */
+#define DIM2D_ERR_WALL_ROOT 5    /* wall ghost-cell root not bracketed / not converged */
+#define DIM2D_ERR_TIMEOUT 6      /* a bounded device wait expired */
+#define DIM2D_ERR_NOT_READY 7    /* state not uploaded yet */
+
+/* boundary choices: src/parameters/parameters_constant.f:145-152 */
+#define DIM2D_PERIODIC_X 0
+#define DIM2D_PERIODIC_Y 1
+#define DIM2D_REFLECTION_X 2
+#define DIM2D_REFLECTION_Y 3
+#define DIM2D_HEDSTROM 4
+#define DIM2D_WALL 7
+/* boundary application types: parameters_constant.f:158-161 */
+#define DIM2D_BC_NODES 0
+#define DIM2D_BC_FLUXES 1
+#define DIM2D_BC_TIMEDEV 2
+#define DIM2D_BC_FLUX_AND_NODE 3
+/* section types used by bc_order: parameters_constant.f:165-172 */
+#define DIM2D_SW_CORNER 1
+#define DIM2D_SE_CORNER 2
+#define DIM2D_NW_CORNER 3
+#define DIM2D_NE_CORNER 4
+#define DIM2D_S_EDGE 5
+#define DIM2D_E_EDGE 6
+#define DIM2D_W_EDGE 7
+#define DIM2D_N_EDGE 8
+/* cardinal slots of the bc_choice / bc_type arrays */
+#define DIM2D_SIDE_N 0
+#define DIM2D_SIDE_S 1
+#define DIM2D_SIDE_E 2
+#define DIM2D_SIDE_W 3
+#define DIM2D_SIDE_NE 4
+#define DIM2D_SIDE_NW 5
+#define DIM2D_SIDE_SE 6
+#define DIM2D_SIDE_SW 7
+
+/* precision of the stencil/flux pass */
+#define DIM2D_FP64 0
+#define DIM2D_MIXED 1 /* FP32 field reads for the flux pass, FP64 accumulation */
+
+/* Physical and boundary constants.  The reference holds these as
+ * compile-time Fortran parameters:
+ *   re, we, pr, cv_r, viscous_r   src/physical_models/dim2d/dim2d_parameters.f:146-199
+ *   gravity_ac, gravity           src/parameters/parameters_input.f:197-202
+ *   wall_*                        src/parameters/parameters_input.f:526-624
+ *   obc_*, T0, flow_velocity      src/parameters/parameters_input.f:127-157,630-662 */
+typedef struct dim2d_params {
+  double re, we, pr, cv_r, viscous_r;
+  int gravity_ac;
+  double gravity;
+  double wall_micro_contact_angle; /* degrees */
+  int wall_heat_source_choice;     /* 0 = no_heat_source */
+  double wall_maximum_heat_flux;
+  double wall_heat_source_center, wall_heat_source_variance;
+  int obc_eigenqties_strategy;     /* 0 = obc_eigenqties_bc */
+  int obc_edge_flux_strategy;      /* 0 = obc_edge_flux_capillarity */
+  double T0, flow_velocity;
+} dim2d_params;
+
+typedef struct dim2d_handle dim2d_handle;
+
+/* Fill *p with the reference's "for tests" constant set
+ * (dim2d_parameters.f:179-187: Re=5, We=10, Pr=20, cv_r=2.5,
+ * viscous_r=-1.5), no gravity, 90 degree contact angle, no heat source. */
+DIM2D_API void dim2d_default_params(dim2d_params *p);
+
+/* Create a solver for one nx x ny field (ghosts included) on the current
+ * CUDA device.  bc_choice/bc_type are indexed by DIM2D_SIDE_*; bc_order
+ * lists the 8 DIM2D_*_EDGE/CORNER section types in node-BC order
+ * (parameters_input.f:397-453).  A periodic domain is bc_choice =
+ * PERIODIC_Y on N/S and PERIODIC_X elsewhere (library_config.py:72-87),
+ * all types DIM2D_BC_NODES; it selects the periodic_xy operator
+ * (src/boundary_conditions/periodic_xy/bc_operators_class.f:116-199).
+ * Allocates three device copies of the field.
+ * Replaces: field%ini + td_integrator selection (field_abstract_class.f:148-198). */
+DIM2D_API int dim2d_create(const dim2d_params *p, int nx, int ny, const int bc_choice[8],
+                 const int bc_type[8], const int bc_order[8], int precision,
+                 dim2d_handle **out);
+
+/* Copy nodes(nx,ny,4), x_map(nx), y_map(ny) and the time to the device.
+ * dx = x_map(2)-x_map(1), dy = y_map(2)-y_map(1) as in
+ * td_operators_class.f:157-158. */
+DIM2D_API int dim2d_upload(dim2d_handle *h, const double *nodes, const double *x_map,
+                 const double *y_map, double t);
+
+/* nsteps calls of field%integrate(dt): three RK3-TVD stages each with
+ * compute_time_dev, the stage update and apply_bc_on_nodes
+ * (td_integrator_class.f:103-161, rk3tvd_steps_module.f:52-490), time += dt. */
+DIM2D_API int dim2d_step(dim2d_handle *h, double dt, int nsteps);
+
+/* time_dev(nx,ny,4) = L(nodes) of the resident state, interior cells (and
+ * the ghost cells of time-derivative boundaries); other cells are written
+ * with debug_real = NF90_FILL_DOUBLE like td_operators_class.f:150-154. */
+DIM2D_API int dim2d_time_dev(dim2d_handle *h, double *time_dev);
+
+/* field%apply_bc_on_nodes on the resident state, with nodes_tmp = nodes
+ * (field_abstract_class.f:190-193). */
+DIM2D_API int dim2d_apply_bc_on_nodes(dim2d_handle *h);
+
+/* Copy the resident state (and time) back to the host; synchronises. */
+DIM2D_API int dim2d_download(dim2d_handle *h, double *nodes, double *t);
+
+/* dt = cfl * min(dx,dy) / max over interior nodes of (c + |u|), speed of
+ * sound from dim2d_prim_module.f:1179-1215, reduced on the device. */
+DIM2D_API int dim2d_cfl_dt(dim2d_handle *h, double cfl, double *dt);
+
+/* Run on the given CUDA stream (cudaStream_t) instead of the handle's own. */
+DIM2D_API int dim2d_set_stream(dim2d_handle *h, void *stream);
+/* Wait for all work queued on the handle. */
+DIM2D_API int dim2d_sync(dim2d_handle *h);
+/* Device pointer of the resident nodes (layout: 4 planes of ny rows of
+ * `pitch` doubles) -- for callers that keep fields in HBM. */
+DIM2D_API int dim2d_device_state(dim2d_handle *h, double **nodes, int *pitch);
+/* Number of kernel launches issued by this handle so far. */
+DIM2D_API long long dim2d_launch_count(const dim2d_handle *h);
+/* Live kernel timing for roofline reports: while enabled, every launch of
+ * the fused interior stage kernel is bracketed by CUDA events on the
+ * handle's stream.  dim2d_profile_read synchronises and returns the summed
+ * device time (ms) and the number of timed launches since enabling. */
+DIM2D_API int dim2d_profile(dim2d_handle *h, int enable);
+DIM2D_API int dim2d_profile_read(dim2d_handle *h, double *ms, long long *launches);
+
+DIM2D_API int dim2d_destroy(dim2d_handle *h);
+
+/* field_abstract_class.f:286-315: dx = (x_max-x_min)/(nx-1-2*bc_size). */
+DIM2D_API int dim2d_ini_coordinates(int nx, int ny, double x_min, double x_max, double y_min,
+                          double y_max, double *x_map, double *y_map);
+
+/* Message of the last error on the calling host thread. */
+DIM2D_API const char *dim2d_last_error(void);
+DIM2D_API const char *dim2d_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,171 @@
+"""ctypes loader for the oracle library (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: the checker for tests/, __graft_entry__.smoke()
+and the CPU-baseline legs of bench.py.  The product never imports this.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+# parameters_constant.f:145-176
+PERIODIC_X, PERIODIC_Y, REFLECTION_X, REFLECTION_Y, HEDSTROM, WALL = 0, 1, 2, 3, 4, 7
+BC_NODES, BC_FLUXES, BC_TIMEDEV, BC_FLUX_AND_NODE = 0, 1, 2, 3
+SW_CORNER, SE_CORNER, NW_CORNER, NE_CORNER, S_EDGE, E_EDGE, W_EDGE, N_EDGE = range(1, 9)
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("re", ctypes.c_double), ("we", ctypes.c_double), ("pr", ctypes.c_double),
+        ("cv_r", ctypes.c_double), ("viscous_r", ctypes.c_double),
+        ("gravity_ac", ctypes.c_int), ("gravity", ctypes.c_double),
+        ("wall_micro_contact_angle", ctypes.c_double),
+        ("wall_heat_source_choice", ctypes.c_int),
+        ("wall_maximum_heat_flux", ctypes.c_double),
+        ("wall_heat_source_center", ctypes.c_double),
+        ("wall_heat_source_variance", ctypes.c_double),
+        ("obc_eigenqties_strategy", ctypes.c_int),
+        ("obc_edge_flux_strategy", ctypes.c_int),
+        ("T0", ctypes.c_double), ("flow_velocity", ctypes.c_double),
+    ]
+
+
+class Cfg(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("periodic", ctypes.c_int),
+        ("bc_choice", ctypes.c_int * 8), ("bc_type", ctypes.c_int * 8),
+        ("bc_order", ctypes.c_int * 8),
+    ]
+
+
+def build():
+    """Compile the oracle (make in this directory)."""
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.orc_sd_operator.restype = ctypes.c_double
+        L.orc_sd_operator.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.orc_flux_function.restype = ctypes.c_double
+        L.orc_flux_function.argtypes = [ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                        ctypes.c_double]
+        L.orc_classical_pressure_local.restype = ctypes.c_double
+        L.orc_classical_pressure_local.argtypes = [_dp]
+        L.orc_speed_of_sound.restype = ctypes.c_double
+        L.orc_speed_of_sound.argtypes = [_dp]
+        L.orc_compute_time_dev.restype = None
+        L.orc_compute_time_dev.argtypes = [ctypes.POINTER(Cfg), ctypes.c_double, _dp, _dp, _dp, _dp]
+        L.orc_apply_bc_on_nodes.restype = None
+        L.orc_apply_bc_on_nodes.argtypes = [ctypes.POINTER(Cfg), ctypes.c_double, _dp, _dp, _dp, _dp]
+        L.orc_integrate.restype = ctypes.c_int
+        L.orc_integrate.argtypes = [ctypes.POINTER(Cfg), _dp, _dp, _dp,
+                                    ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.c_int]
+        L.orc_ini_coordinates.restype = None
+        L.orc_ini_coordinates.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 4 + [_dp, _dp]
+        L.orc_set_params.argtypes = [ctypes.POINTER(Params)]
+        L.orc_get_params.argtypes = [ctypes.POINTER(Params)]
+        L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_debug_real.restype = ctypes.c_double
+        _lib = L
+    return _lib
+
+
+def ptr(a):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+def get_params():
+    p = Params()
+    lib().orc_get_params(ctypes.byref(p))
+    return p
+
+
+def set_params(**kw):
+    p = get_params()
+    for k, v in kw.items():
+        setattr(p, k, v)
+    lib().orc_set_params(ctypes.byref(p))
+    return p
+
+
+def set_threads(n):
+    lib().orc_set_threads(int(n))
+
+
+def make_cfg(nx, ny, periodic=False, bc_choice=None, bc_type=None, bc_order=None):
+    c = Cfg()
+    c.nx, c.ny, c.periodic = nx, ny, int(bool(periodic))
+    for k in range(8):
+        c.bc_choice[k] = (bc_choice or [0] * 8)[k]
+        c.bc_type[k] = (bc_type or [0] * 8)[k]
+        c.bc_order[k] = (bc_order or list(range(1, 9)))[k]
+    return c
+
+
+def ini_coordinates(nx, ny, x_min, x_max, y_min, y_max):
+    x = np.zeros(nx)
+    y = np.zeros(ny)
+    lib().orc_ini_coordinates(nx, ny, x_min, x_max, y_min, y_max, ptr(x), ptr(y))
+    return x, y
+
+
+def compute_time_dev(cfg, t, nodes, x_map, y_map):
+    """nodes: C array [4][ny][nx] (Fortran nodes(nx,ny,4))."""
+    nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+    td = np.empty_like(nodes)
+    lib().orc_compute_time_dev(ctypes.byref(cfg), t, ptr(nodes), ptr(x_map), ptr(y_map), ptr(td))
+    return td
+
+
+def apply_bc_on_nodes(cfg, t, x_map, y_map, nodes_tmp, nodes):
+    lib().orc_apply_bc_on_nodes(ctypes.byref(cfg), t, ptr(x_map), ptr(y_map), ptr(nodes_tmp),
+                                ptr(nodes))
+
+
+def integrate(cfg, nodes, x_map, y_map, t, dt, nsteps):
+    """Advance nodes in place by nsteps RK3 steps; returns the new time."""
+    tt = ctypes.c_double(t)
+    rc = lib().orc_integrate(ctypes.byref(cfg), ptr(nodes), ptr(x_map), ptr(y_map),
+                             ctypes.byref(tt), dt, nsteps)
+    if rc != 0:
+        raise RuntimeError("oracle integrate failed: %d" % rc)
+    return tt.value
+
+
+def sd_operator(set_id, op, nodes, i, j, dx, dy):
+    nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+    ny, nx = nodes.shape[1], nodes.shape[2]
+    return lib().orc_sd_operator(set_id, op, ptr(nodes), nx, ny, i, j, dx, dy)
+
+
+def flux_function(which, nodes, i, j, dx, dy):
+    nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+    ny, nx = nodes.shape[1], nodes.shape[2]
+    return lib().orc_flux_function(which, ptr(nodes), nx, ny, i, j, dx, dy)
+
+
+def pressure(q):
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    return lib().orc_classical_pressure_local(ptr(q))
+
+
+def speed_of_sound(q):
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    return lib().orc_speed_of_sound(ptr(q))
