@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--n", type=int, default=N_INTERIOR)
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--bc", default="periodic_xy")
+    ap.add_argument("--cpu-budget", type=float, default=15.0,
+                    help="seconds of host time for the cpu_baseline sample")
     return ap.parse_args()
 
 
@@ -318,7 +320,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
-        line["cpu_baseline"] = cpu_baseline(w)
+        line["cpu_baseline"] = cpu_baseline(w, budget_s=a.cpu_budget)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

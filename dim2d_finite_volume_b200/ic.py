@@ -115,12 +115,17 @@ def bubbles(x_map, y_map, T0, bubbles_xyr, li, velocity=(0.0, 0.0), we=10.0, cv_
 
 
 def cfl_dt(q, dx, dy, cfl, cv_r=2.5):
-    """dt = CFL*min(dx,dy)/max(c+|u|) over the interior nodes."""
+    """dt = CFL*min(dx,dy)/max(c+|u|) over the interior nodes.
+
+    Nodes where the speed of sound is undefined (spinodal states, where
+    the square roots of dim2d_prim_module.f:1197-1202 have negative
+    arguments) are skipped, like fmax skips NaN in the device reduction."""
     s = (slice(None), slice(BC_SIZE, -BC_SIZE), slice(BC_SIZE, -BC_SIZE))
     qi = q[s]
-    c = sound_speed(qi[0], qi[1], qi[2], qi[3], cv_r)
+    with np.errstate(invalid="ignore"):
+        c = sound_speed(qi[0], qi[1], qi[2], qi[3], cv_r)
     u = np.sqrt((qi[1] / qi[0]) ** 2 + (qi[2] / qi[0]) ** 2)
-    return cfl * min(dx, dy) / float(np.max(c + u))
+    return cfl * min(dx, dy) / float(np.nanmax(c + u))
 
 
 def config1(n=128, T0=0.95, radius=0.1, cfl=0.1, cv_r=2.5, we=10.0):

@@ -9,13 +9,6 @@
 
 #include "dim2d_oracle_internal.h"
 
-const sd_ops *orc_sd_set(int set) {
-  switch (set) {
-    case 0: return &SD_INTERIOR;
-  }
-  return NULL;
-}
-
 /* bc_operators_gen_class.f:238-407: walk bc_order1..8 and apply the
  * node-type operators of each section */
 void orc_bc_gen_apply_on_nodes(const orc_cfg *c, double t, const double *x_map,
