@@ -1,0 +1,137 @@
+// dim2d_noalloc.cu -- dim2d_step_noalloc: the RK3 time step without any
+// device allocation.
+//
+// dim2d_step keeps its two RK3 stage copies in buffers that dim2d_create
+// obtains with cudaMalloc.  Some callers cannot allocate device memory:
+// hosts that hand every byte of HBM out from their own pool or arena (a
+// serving loop that pre-sizes memory for admitted requests, a Fortran
+// code whose arrays live in CUDA-Fortran or OpenACC managed storage), and
+// time-stepping loops that must not allocate because cudaMalloc
+// synchronises the device.  For them this entry point takes the field as
+// a device pointer and runs the same stage kernels with the stage copies
+// placed in one file-scope __device__ array of fixed size.
+//
+// Limits and sharing rules (also stated in include/dim2d.h):
+//   * at most DIM2D_NOALLOC_MAX_CELLS = nx*ny cells (ghosts included);
+//     the array holds 2 x 4 x that many doubles (16 MiB) on every GPU
+//     that loads the library, until the process exits;
+//   * every call on a device uses the same array, which keeps the last
+//     call's contents: each call clears the part it uses before stepping,
+//     and calls that overlap on the GPU (different streams, or host
+//     threads not ordered by the caller) race on it;
+//   * the first call on a device, with that device current, looks up the
+//     array's device address once (cudaGetSymbolAddress); make that first
+//     call before any stream capture.
+#include <cmath>
+#include <mutex>
+
+#include "dim2d_internal.h"
+
+using namespace dim2d;
+
+namespace {
+
+constexpr size_t kMaxCells = DIM2D_NOALLOC_MAX_CELLS;
+constexpr size_t kScratchDoubles = 2 * 4 * kMaxCells;
+constexpr int kMaxDevices = 64;
+
+// Two stage copies of the field; only device code and the looked-up
+// address below may touch it (in host code the name is a host-side
+// stand-in, not a device address).
+__device__ __align__(256) double g_stage_scratch[kScratchDoubles];
+
+std::mutex g_scratch_mu;
+double* g_scratch_addr[kMaxDevices] = {};
+
+int scratch_address(double** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_error(e, "step_noalloc: cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices)
+    return set_error(DIM2D_ERR_ARG, "step_noalloc: device %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_stage_scratch);
+    if (e != cudaSuccess || !p)
+      return cuda_error(e == cudaSuccess ? cudaErrorInvalidSymbol : e,
+                        "step_noalloc: cudaGetSymbolAddress");
+    g_scratch_addr[dev] = static_cast<double*>(p);
+  }
+  *out = g_scratch_addr[dev];
+  return DIM2D_OK;
+}
+
+}  // namespace
+
+extern "C" int dim2d_step_noalloc(const dim2d_params* p, int nx, int ny, const int bc_choice[8],
+                                  const int bc_type[8], const int bc_order[8], double* nodes,
+                                  const double* x_map, const double* y_map, double dt,
+                                  int nsteps, void* stream) {
+  if (!p || !bc_choice || !bc_type || !bc_order || !nodes || !x_map || !y_map)
+    return set_error(DIM2D_ERR_ARG, "step_noalloc: null argument");
+  if (nx < 8 || ny < 8)
+    return set_error(DIM2D_ERR_ARG, "step_noalloc: nx, ny must be >= 8 (got %d x %d)", nx, ny);
+  if ((size_t)nx * (size_t)ny > kMaxCells)
+    return set_error(DIM2D_ERR_ARG,
+                     "step_noalloc: nx*ny = %zu exceeds the fixed scratch limit of %zu cells "
+                     "(DIM2D_NOALLOC_MAX_CELLS); use dim2d_create/dim2d_step for larger fields",
+                     (size_t)nx * (size_t)ny, kMaxCells);
+  if (nsteps < 0 || !std::isfinite(dt)) return set_error(DIM2D_ERR_ARG, "step_noalloc: bad dt/nsteps");
+  if (!(p->re > 0) || !(p->we > 0) || !(p->pr > 0) || !(p->cv_r > 0))
+    return set_error(DIM2D_ERR_ARG, "step_noalloc: re, we, pr, cv_r must be positive");
+  int side_kind[8], periodic = 0;
+  int rc = resolve_sides(bc_choice, bc_type, side_kind, &periodic);
+  if (rc) return rc;
+  if (!periodic)
+    return set_error(DIM2D_ERR_UNSUPPORTED,
+                     "step_noalloc: configuration not provided (same set as dim2d_create)");
+  const double dx = x_map[1] - x_map[0], dy = y_map[1] - y_map[0];
+  if (!(dx > 0) || !(dy > 0)) return set_error(DIM2D_ERR_ARG, "step_noalloc: x_map/y_map not increasing");
+
+  double* scratch = nullptr;
+  rc = scratch_address(&scratch);
+  if (rc) return rc;
+
+  // a handle on the stack that owns nothing: A = the caller's field,
+  // B and C = the two halves of the static scratch
+  dim2d_handle h;
+  h.p = *p;
+  h.k = make_const(*p);
+  h.precision = DIM2D_FP64;
+  h.periodic = periodic;
+  for (int s = 0; s < 8; s++) {
+    h.bc_choice[s] = bc_choice[s];
+    h.bc_type[s] = bc_type[s];
+    h.bc_order[s] = bc_order[s];
+    h.side_kind[s] = side_kind[s];
+  }
+  h.f.nx = nx;
+  h.f.ny = ny;
+  h.f.pitch = nx;  // the caller's Fortran layout
+  h.f.plane = (size_t)nx * ny;
+  h.A = nodes;
+  h.B = scratch;
+  h.C = scratch + 4 * h.f.plane;
+  h.dx = dx;
+  h.dy = dy;
+  h.rdx = 1.0 / dx;
+  h.rdy = 1.0 / dy;
+  h.uploaded = true;
+  h.stream = static_cast<cudaStream_t>(stream);
+
+  // the array keeps the previous call's contents: start from zeros
+  cudaError_t e = cudaMemsetAsync(scratch, 0, 2 * 4 * h.f.plane * sizeof(double), h.stream);
+  if (e != cudaSuccess) return cuda_error(e, "step_noalloc: clear scratch");
+  for (int s = 0; s < nsteps; s++) {
+    rc = rk3_step(&h, dt);
+    if (rc) return rc;
+  }
+  // after an odd number of steps the newest state sits in the scratch
+  if (h.A != nodes) {
+    e = cudaMemcpyAsync(nodes, h.A, 4 * h.f.plane * sizeof(double), cudaMemcpyDeviceToDevice,
+                        h.stream);
+    if (e != cudaSuccess) return cuda_error(e, "step_noalloc: copy back");
+  }
+  return DIM2D_OK;
+}
