@@ -19,6 +19,7 @@ SOURCES = [
     "dim2d_step.cu",
     "dim2d_interior.cu",
     "dim2d_noalloc.cu",
+    "dim2d_open.cu",
 ]
 HEADERS = ["dim2d_physics.cuh", "dim2d_kernels.cuh", "dim2d_internal.h"]
 

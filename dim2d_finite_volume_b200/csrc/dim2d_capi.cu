@@ -84,6 +84,12 @@ int resolve_sides(const int bc_choice[8], const int bc_type[8], int side_kind[8]
   return DIM2D_OK;
 }
 
+int all_open(const int bc_choice[8], const int bc_type[8]) {
+  for (int s = 0; s < 8; s++)
+    if (bc_choice[s] != DIM2D_HEDSTROM || bc_type[s] != DIM2D_BC_TIMEDEV) return 0;
+  return 1;
+}
+
 }  // namespace dim2d
 
 extern "C" {
@@ -140,9 +146,11 @@ int dim2d_create(const dim2d_params* p, int nx, int ny, const int bc_choice[8],
   int side_kind[8], periodic = 0;
   int rc = resolve_sides(bc_choice, bc_type, side_kind, &periodic);
   if (rc) return rc;
-  if (!periodic)
+  const int open = all_open(bc_choice, bc_type);
+  if (!periodic && !open)
     return set_error(DIM2D_ERR_UNSUPPORTED,
-                     "create: only the periodic_xy configuration is provided by this build");
+                     "create: boundary configuration not provided (periodic_xy and hedstrom_xy "
+                     "are)");
   if (precision != DIM2D_FP64)
     return set_error(DIM2D_ERR_UNSUPPORTED, "create: mixed precision not provided by this build");
 
@@ -151,6 +159,7 @@ int dim2d_create(const dim2d_params* p, int nx, int ny, const int bc_choice[8],
   h->k = make_const(*p);
   h->precision = precision;
   h->periodic = periodic;
+  h->open_all = open;
   std::memcpy(h->bc_choice, bc_choice, sizeof h->bc_choice);
   std::memcpy(h->bc_type, bc_type, sizeof h->bc_type);
   std::memcpy(h->bc_order, bc_order, sizeof h->bc_order);
@@ -314,6 +323,19 @@ int dim2d_time_dev(dim2d_handle* h, double* time_dev) {
   h->launches++;
   if (e == cudaSuccess) {
     e = launch_time_dev(h->A, h->td, f, h->rdx, h->rdy, h->k, h->stream);
+    h->launches++;
+  }
+  if (e == cudaSuccess && h->open_all) {
+    // bc_operators_hedstrom_xy_class.f:182-496: ghost-cell time derivatives
+    StageArgs a{};
+    a.uin = h->A;
+    a.u0 = h->A;
+    a.uout = h->td;
+    a.f = f;
+    a.rdx = h->rdx;
+    a.rdy = h->rdy;
+    a.k = h->k;
+    e = launch_open_ghosts(a, 0, h->stream);
     h->launches++;
   }
   if (e != cudaSuccess) return cuda_error(e, "time_dev");

@@ -14,6 +14,7 @@ struct dim2d_handle {
   dim2d::DimConst k{};
   int precision = 0;
   int periodic = 0;
+  int open_all = 0;  // hedstrom_xy: every section open, type bc_timedev
   int bc_choice[8]{}, bc_type[8]{}, bc_order[8]{};
   int side_kind[8]{};
   dim2d::Field f{};
@@ -47,6 +48,8 @@ int cuda_error(cudaError_t e, const char* where);
 DimConst make_const(const dim2d_params& p);
 int pitch_for(int nx);
 int resolve_sides(const int bc_choice[8], const int bc_type[8], int side_kind[8], int* periodic);
+// 1 if all eight sections are hedstrom_choice with type bc_timedev
+int all_open(const int bc_choice[8], const int bc_type[8]);
 }  // namespace dim2d
 
 // dim2d_step.cu

@@ -40,6 +40,9 @@ size_t interior_smem_bytes();
 cudaError_t launch_interior_stage(const StageArgs& a, cudaStream_t s);
 cudaError_t launch_time_dev(const double* uin, double* td, const Field& f, double rdx, double rdy,
                             const DimConst& k, cudaStream_t s);
+// open (Hedstrom) ghost cells of a field open on all sides; mode 0 writes
+// L(u) into a.uout, mode 1 the RK stage update
+cudaError_t launch_open_ghosts(const StageArgs& a, int mode, cudaStream_t s);
 cudaError_t launch_fill(double* p, double v, size_t n, cudaStream_t s);
 cudaError_t launch_periodic_ghosts(double* u, const Field& f, cudaStream_t s);
 cudaError_t launch_cfl_max(const double* u, const Field& f, const DimConst& k, double* out,

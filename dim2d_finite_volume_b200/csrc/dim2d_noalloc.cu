@@ -83,9 +83,10 @@ extern "C" int dim2d_step_noalloc(const dim2d_params* p, int nx, int ny, const i
   int side_kind[8], periodic = 0;
   int rc = resolve_sides(bc_choice, bc_type, side_kind, &periodic);
   if (rc) return rc;
-  if (!periodic)
+  const int open = all_open(bc_choice, bc_type);
+  if (!periodic && !open)
     return set_error(DIM2D_ERR_UNSUPPORTED,
-                     "step_noalloc: configuration not provided (same set as dim2d_create)");
+                     "step_noalloc: configuration not provided (periodic_xy and hedstrom_xy are)");
   const double dx = x_map[1] - x_map[0], dy = y_map[1] - y_map[0];
   if (!(dx > 0) || !(dy > 0)) return set_error(DIM2D_ERR_ARG, "step_noalloc: x_map/y_map not increasing");
 
@@ -100,6 +101,7 @@ extern "C" int dim2d_step_noalloc(const dim2d_params* p, int nx, int ny, const i
   h.k = make_const(*p);
   h.precision = DIM2D_FP64;
   h.periodic = periodic;
+  h.open_all = open;
   for (int s = 0; s < 8; s++) {
     h.bc_choice[s] = bc_choice[s];
     h.bc_type[s] = bc_type[s];

@@ -21,6 +21,7 @@ int apply_bc_on_nodes(dim2d_handle* h, const double* nodes_tmp, double* nodes) {
     if (e != cudaSuccess) return cuda_error(e, "apply_bc_on_nodes(periodic)");
     return DIM2D_OK;
   }
+  if (h->open_all) return DIM2D_OK;  // no section of node type
   return set_error(DIM2D_ERR_UNSUPPORTED, "apply_bc_on_nodes: configuration not provided");
 }
 
@@ -70,8 +71,17 @@ static int stage(dim2d_handle* h, int st, const double* uin, double* uout, doubl
   prof_end(h);
   h->launches++;
   if (e != cudaSuccess) return cuda_error(e, "rk3 stage");
-  if (!h->periodic) return apply_bc_on_nodes(h, h->A, uout);
-  return DIM2D_OK;
+  if (h->periodic) return DIM2D_OK;  // ghost images written by the stage kernel
+  if (h->open_all) {
+    // every ghost cell has a time derivative and is integrated like the
+    // interior (x/y_borders widened, field_abstract_class.f:244-270); no
+    // node boundary pass follows
+    e = launch_open_ghosts(a, 1, h->stream);
+    h->launches++;
+    if (e != cudaSuccess) return cuda_error(e, "rk3 stage (open ghosts)");
+    return DIM2D_OK;
+  }
+  return apply_bc_on_nodes(h, h->A, uout);
 }
 
 int rk3_step(dim2d_handle* h, double dt) {

@@ -77,6 +77,13 @@ double orc_sd_operator(int set, int op, const double *nodes, int nx, int ny,
  * test_lernaeanhydra/test_dim2d_fluxes.f:291-316 (1-based) */
 double orc_flux_function(int which, const double *nodes, int nx, int ny,
                          int i, int j, double dx, double dy);
+/* hedstrom_xy_module.f:445-558 at node (i,j): direction 0 = x, 1 = y;
+ * oneside_right selects the R0 (else L0) one-sided gradient; side_right
+ * the incoming-wave test of a right (E/N) side; obc_prim = the 5
+ * eigen-quantities (rho,u,v,P,c) or NULL for obc_eigenqties_bc. */
+void orc_timedev_with_openbc(const double *nodes, int nx, int ny, int i, int j, int dir_y,
+                             int oneside_right, double dn, int side_right,
+                             const double *obc_prim, double td[4]);
 /* primitive helpers */
 double orc_classical_pressure_local(const double q[4]);
 double orc_speed_of_sound(const double q[4]);

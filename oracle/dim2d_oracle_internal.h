@@ -115,6 +115,14 @@ void orc_bc_apply_on_fluxes(const orc_cfg *c, double t, const double *x_map, con
                             const ov *n, double dx, double dy, double *flux_x, double *flux_y);
 void orc_bc_apply_on_timedev(const orc_cfg *c, double t, const double *x_map,
                              const double *y_map, const ov *n, double dx, double dy,
-                             const double *flux_x, const double *flux_y, double *time_dev);
+                             double *flux_x, double *flux_y, double *time_dev);
+/* section bounds [type, i_min, j_min, i_max/j_max] (bc_operators_gen_class.f:95-102) */
+void orc_section(const orc_cfg *c, int section, int sec[4]);
+void orc_reflection_apply_on_nodes(const orc_cfg *c, int section, int choice, double *nodes);
+void orc_wall_apply_on_nodes(const orc_cfg *c, int section, double t, const double *x_map,
+                             const double *y_map, const double *nodes_tmp, double *nodes);
+void orc_wall_apply_on_fluxes(const orc_cfg *c, int section, double t, const double *x_map,
+                              const double *y_map, const ov *n, double dx, double dy,
+                              double *flux_x, double *flux_y);
 
 #endif

@@ -169,3 +169,21 @@ def pressure(q):
 def speed_of_sound(q):
     q = np.ascontiguousarray(q, dtype=np.float64)
     return lib().orc_speed_of_sound(ptr(q))
+
+
+def timedev_with_openbc(nodes, i, j, dir_y, oneside_right, dn, side_right, obc_prim=None):
+    """hedstrom_xy_module.f:445-558 at node (i,j) (1-based)."""
+    L = lib()
+    fn = L.orc_timedev_with_openbc
+    fn.restype = None
+    fn.argtypes = [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                   ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp, _dp]
+    nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+    ny, nx = nodes.shape[1], nodes.shape[2]
+    td = np.zeros(4)
+    pp = None
+    if obc_prim is not None:
+        pp = np.ascontiguousarray(obc_prim, dtype=np.float64)
+    fn(ptr(nodes), nx, ny, i, j, int(dir_y), int(oneside_right), dn, int(side_right),
+       ptr(pp) if pp is not None else None, ptr(td))
+    return td

@@ -145,11 +145,72 @@ def dim2d_fluxes(ref):
     }
 
 
+def _reshape_blocks(text, ne):
+    """All `reshape((/ ... /),(/a,b,c/))` literals of a Fortran text, in order
+    (`ne` stands for the number of equations of that test)."""
+    out = []
+    for m in re.finditer(r"reshape\(\(/(.*?)/\)[\s$]*,[\s$]*\(/([\w,\s]+)/\)\)", text, re.S):
+        body = re.sub(r"\n\s*\$", " ", m.group(1))
+        if "=" in body:  # implied-do constructors are generated, not literal
+            continue
+        vals = [fnum(t) for t in re.findall(NUM, body)]
+        shape = [ne if s.strip() == "ne" else int(s) for s in m.group(2).split(",")]
+        out.append({"values": vals, "shape": shape})
+    return out
+
+
+def hedstrom(ref):
+    """test_bc_operators/test_hedstrom_xy.f:54-178."""
+    path = os.path.join(ref, "src/test_files/test_bc_operators/test_hedstrom_xy.f")
+    src = open(path).read()
+    blocks = _reshape_blocks(src, 4)
+    nodes_L0, nodes_R0 = blocks[0], blocks[1]
+    vecs = re.findall(r"\[([^\]]*)\]", src)
+    vecs = [[fnum(t) for t in re.findall(NUM, re.sub(r"\n\s*\$", " ", v))] for v in vecs]
+    vecs = [v for v in vecs if len(v) in (4, 5)]
+    td_L0, td_R0 = [v for v in vecs if len(v) == 4][:2]
+    obc = [v for v in vecs if len(v) == 5]
+    dx = fnum(re.search(r"\bdx\s*=\s*(%s)" % NUM, src).group(1))
+    return {
+        "source": "src/test_files/test_bc_operators/test_hedstrom_xy.f",
+        "note": "obc_eigenqties_lin: the 5 far-field eigen-quantities (rho,u,v,P,c) are the "
+                "values get_prim_obc_eigenqties must return in the same test",
+        "nodes_L0": nodes_L0, "nodes_R0": nodes_R0, "i_L0": 1, "i_R0": 3, "j": 1,
+        "dx": dx, "cv_r": 2.5,
+        "obc_prim": obc[-1], "obc_prim_input": obc[0] if len(obc) > 1 else None,
+        "timedev_L0": td_L0, "timedev_R0": td_R0,
+    }
+
+
+def periodic(ref):
+    """test_bc_operators/test_periodic_xy.f:94-190: nodes(i,j,k) =
+    (i-1)+8(j-1)+100(k-1) on 8x10x3 and the expected ghost blocks."""
+    path = os.path.join(ref, "src/test_files/test_bc_operators/test_periodic_xy.f")
+    src = open(path).read()
+    body = src[src.index("function test_apply_bc_on_nodes("):]
+    body = body[:body.index("end function test_apply_bc_on_nodes")]
+    targets = re.findall(r"test_nodes\((\d+):(\d+),(\d+):(\d+),:\)\s*=", body)
+    blocks = _reshape_blocks(body, 3)
+    assert len(targets) == len(blocks) == 4, (len(targets), len(blocks))
+    out = []
+    for (i0, i1, j0, j1), b in zip(targets, blocks):
+        out.append({"i": [int(i0), int(i1)], "j": [int(j0), int(j1)], "shape": b["shape"],
+                    "values": b["values"]})
+    return {
+        "source": "src/test_files/test_bc_operators/test_periodic_xy.f",
+        "nx": 8, "ny": 10, "ne": 3,
+        "nodes_formula": "(i-1)+8*(j-1)+100*(k-1), 1-based i,j,k",
+        "expected_blocks": out,
+    }
+
+
 def main():
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     out = {
         "mattsson_operators.json": mattsson(ref),
         "dim2d_fluxes.json": dim2d_fluxes(ref),
+        "hedstrom_xy.json": hedstrom(ref),
+        "periodic_xy.json": periodic(ref),
     }
     for name, obj in out.items():
         with open(os.path.join(HERE, name), "w") as fh:

@@ -79,3 +79,39 @@ def test_dim2d_flux_known_answers(oracle):
             bad.append((k, v, e["literal"]))
     assert not bad, bad
     assert len(f["expected"]) == 26
+
+
+def _fortran_array(block):
+    """reshape((/values/),(/a,b,c/)) -> C array [c][b][a]."""
+    a, b, c = block["shape"]
+    return np.array(block["values"]).reshape(c, b, a)
+
+
+def test_hedstrom_characteristic_known_answers(oracle):
+    """compute_timedev_with_openbc at an L0 and an R0 node
+    (test_bc_operators/test_hedstrom_xy.f:54-136), far-field eigen-quantities."""
+    h = json.load(open(os.path.join(GOLD, "hedstrom_xy.json")))
+    oracle.set_params(cv_r=h["cv_r"])
+    nL = _fortran_array(h["nodes_L0"])
+    nR = _fortran_array(h["nodes_R0"])
+    tdL = oracle.timedev_with_openbc(nL, h["i_L0"], h["j"], 0, 0, h["dx"], 0, h["obc_prim"])
+    tdR = oracle.timedev_with_openbc(nR, h["i_R0"], h["j"], 0, 1, h["dx"], 1, h["obc_prim"])
+    np.testing.assert_allclose(tdL, h["timedev_L0"], rtol=0, atol=1e-8)
+    np.testing.assert_allclose(tdR, h["timedev_R0"], rtol=0, atol=1e-10)
+
+
+def test_periodic_ghost_known_answers(oracle):
+    """periodic_xy legacy operator on nodes(i,j,k) = (i-1)+8(j-1)+100(k-1)
+    (test_bc_operators/test_periodic_xy.f:94-190): ghosts bit-exact."""
+    p = json.load(open(os.path.join(GOLD, "periodic_xy.json")))
+    nx, ny = p["nx"], p["ny"]
+    k, j, i = np.meshgrid(np.arange(4), np.arange(ny), np.arange(nx), indexing="ij")
+    nodes = (i + 8 * j + 100 * k).astype(np.float64)
+    cfg = oracle.make_cfg(nx, ny, periodic=True)
+    x = np.arange(nx, dtype=np.float64)
+    y = np.arange(ny, dtype=np.float64)
+    oracle.apply_bc_on_nodes(cfg, 0.0, x, y, nodes.copy(), nodes)
+    for b in p["expected_blocks"]:
+        want = _fortran_array(b)  # [k][j][i] for the block
+        got = nodes[:3, b["j"][0] - 1:b["j"][1], b["i"][0] - 1:b["i"][1]]
+        assert np.array_equal(got, want), b
