@@ -43,29 +43,49 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=N_INTERIOR)
     ap.add_argument("--seed", type=int, default=1234)
-    ap.add_argument("--bc", default="periodic_xy")
+    ap.add_argument("--bc", default="hedstrom_xy", choices=["hedstrom_xy", "periodic_xy"])
     ap.add_argument("--cpu-budget", type=float, default=15.0,
                     help="seconds of host time for the cpu_baseline sample")
     return ap.parse_args()
 
 
-def workload(n, seed, rank=0):
+def workload(n, seed, rank=0, bc="hedstrom_xy"):
+    """The 1024^2 plain FP64 configuration: a bubble of seeded radius in
+    [0.05, 0.15] at T0 = 0.95, carried by a uniform x-flow at Mach 0.1 of
+    the liquid sound speed, open (Hedstrom) boundaries on all sides.
+    With bc='periodic_xy' the same bubble sits still in a periodic box."""
     from dim2d_finite_volume_b200 import ic
     rng = np.random.default_rng(seed + rank)
     nx, ny, x_map, y_map = ic.grid(n)
     dx = x_map[1] - x_map[0]
     r = float(rng.uniform(0.05, 0.15))
-    q = ic.bubbles(x_map, y_map, 0.95, [(0.0, 0.0, r)], li=4.0 * dx)
-    # periodic ghosts as field%ini leaves them
-    px, py = nx - 4, ny - 4
-    q[:, :, 0:2] = q[:, :, px:px + 2]
-    q[:, :, nx - 2:] = q[:, :, 2:4]
-    q[:, 0:2, :] = q[:, py:py + 2, :]
-    q[:, ny - 2:, :] = q[:, 2:4, :]
+    T0 = 0.95
+    u0 = 0.0
+    if bc == "hedstrom_xy":
+        rv, rl = ic.maxwell_densities(T0)
+        e = rl * (8.0 / 3.0 * 2.5 * T0 - 3.0 * rl)
+        u0 = 0.1 * float(ic.sound_speed(np.array(rl), np.array(0.0), np.array(0.0),
+                                        np.array(e), 2.5))
+    q = ic.bubbles(x_map, y_map, T0, [(0.0, 0.0, r)], li=4.0 * dx, velocity=(u0, 0.0))
+    if bc == "periodic_xy":  # periodic ghosts as field%ini leaves them
+        px, py = nx - 4, ny - 4
+        q[:, :, 0:2] = q[:, :, px:px + 2]
+        q[:, :, nx - 2:] = q[:, :, 2:4]
+        q[:, 0:2, :] = q[:, py:py + 2, :]
+        q[:, ny - 2:, :] = q[:, 2:4, :]
     rho_min = float(q[0].min())
     dt = min(ic.cfl_dt(q, dx, dx, 0.1), 0.2 * 5.0 * rho_min * dx * dx)
     return dict(nx=nx, ny=ny, x_map=x_map, y_map=y_map, nodes=np.ascontiguousarray(q), dt=dt,
-                radius=r)
+                radius=r, u0=u0, bc=bc)
+
+
+def oracle_cfg(O, bc, nx, ny):
+    if bc == "periodic_xy":
+        return O.make_cfg(nx, ny, periodic=True)
+    from dim2d_finite_volume_b200 import field as F
+    bc_choice, bc_type, bc_order = F._preset(bc)
+    return O.make_cfg(nx, ny, periodic=False, bc_choice=bc_choice, bc_type=bc_type,
+                      bc_order=bc_order)
 
 
 def measured_peaks():
@@ -137,6 +157,17 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def band_sample(w, rows):
+    """Rows [c - rows/2, c + rows/2) of the field around its centre line,
+    plus ghosts: the same per-cell work as the full field, bounded."""
+    ny = w["ny"]
+    c = ny // 2
+    lo = max(0, c - rows // 2 - 2)
+    hi = lo + rows + 4
+    q = np.ascontiguousarray(w["nodes"][:, lo:hi, :])
+    return q, np.ascontiguousarray(w["y_map"][lo:hi])
+
+
 def cpu_baseline(w, budget_s=15.0, threads=None):
     """Oracle (CPU restatement) on a bounded sample: full RK3 steps of a
     row band of the same field, repeated until budget_s of host time."""
@@ -144,10 +175,9 @@ def cpu_baseline(w, budget_s=15.0, threads=None):
     nth = threads or os.cpu_count() or 1
     O.set_threads(nth)
     nx = w["nx"]
-    band = 64 + 4  # 64 interior rows + ghosts, periodic in y
-    q = np.ascontiguousarray(w["nodes"][:, :band, :])
-    y_map = w["y_map"][:band]
-    cfg = O.make_cfg(nx, band, periodic=True)
+    q, y_map = band_sample(w, 64)
+    band = q.shape[1]
+    cfg = oracle_cfg(O, w["bc"], nx, band)
     O.apply_bc_on_nodes(cfg, 0.0, w["x_map"], y_map, q.copy(), q)
     cells = (nx - 4) * (band - 4)
     steps, t0 = 0, time.perf_counter()
@@ -159,22 +189,22 @@ def cpu_baseline(w, budget_s=15.0, threads=None):
         if el >= budget_s:
             break
     return {"value": cells * steps / el, "unit": "cell-updates/s", "cores": nth, "kind": "port",
-            "sample": "%d RK3 steps of a %dx%d periodic band (interior %dx%d) of the %d^2 "
-                      "field, %.1f s" % (steps, nx, band, nx - 4, band - 4, nx - 4, el)}
+            "sample": "%d RK3 steps of a %dx%d %s band (interior %dx%d) through the centre of "
+                      "the %d^2 field, %.1f s" % (steps, nx, band, w["bc"], nx - 4, band - 4,
+                                                  nx - 4, el)}
 
 
 def run_reference(a, rank, world):
     if rank != 0:
         return
     from oracle import oracle as O
-    w = workload(a.n, a.seed)
+    w = workload(a.n, a.seed, bc=a.bc)
     nth = os.cpu_count() or 1
     O.set_threads(nth)
     nx = w["nx"]
-    band = 32 + 4
-    q = np.ascontiguousarray(w["nodes"][:, :band, :])
-    y_map = w["y_map"][:band]
-    cfg = O.make_cfg(nx, band, periodic=True)
+    q, y_map = band_sample(w, 32)
+    band = q.shape[1]
+    cfg = oracle_cfg(O, a.bc, nx, band)
     O.apply_bc_on_nodes(cfg, 0.0, w["x_map"], y_map, q.copy(), q)
     cells = (nx - 4) * (band - 4)
     t = 0.0
@@ -191,7 +221,7 @@ def run_reference(a, rank, world):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "impl": "reference",
         "config": {"workload": "plain FP64 DIM %d^2 field, RK3 step, row-band sample" % a.n,
-                   "sample_rows": band - 4, "bc": "periodic_xy"},
+                   "sample_rows": band - 4, "bc": a.bc},
         "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": nth, "kind": "port",
                          "sample": "each step: one RK3 step of a %dx%d band of the %d^2 field"
                                    % (nx, band, a.n)},
@@ -221,7 +251,7 @@ def main():
 
     from dim2d_finite_volume_b200 import field as F
 
-    w = workload(a.n, a.seed, rank)
+    w = workload(a.n, a.seed, rank, bc=a.bc)
     nx, ny = w["nx"], w["ny"]
     cells = (nx - 4) * (ny - 4)
     dt = w["dt"]
@@ -302,8 +332,9 @@ def main():
             "n_gpus": world, "steps": a.steps, "warmup": max(3, a.warmup),
             "ms_per_step": step_ms / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "plain FP64 DIM %d^2 (+2 ghosts) bubble, T0=0.95, RK3 step"
-                                   % a.n, "bc": a.bc, "nx": nx, "ny": ny, "dt": dt,
+            "config": {"workload": "plain FP64 DIM %d^2 (+2 ghosts) bubble, T0=0.95, "
+                                   "Mach %.1f flow, RK3 step" % (a.n, 0.1 if a.bc == "hedstrom_xy"
+                                                                 else 0.0), "bc": a.bc, "nx": nx, "ny": ny, "dt": dt,
                        "l2": "flushed between timed steps (2x L2 write, outside the events)",
                        "replicas_per_gpu": 1},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

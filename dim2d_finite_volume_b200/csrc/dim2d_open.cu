@@ -20,6 +20,14 @@
 // the same RK3 stage update as the interior kernel.
 #include "dim2d_kernels.cuh"
 
+#ifdef __CUDA_ARCH__
+#define DIM2D_LDG(p) __ldg(p)
+#elif defined(DIM2D_LDG_HOST)
+#define DIM2D_LDG(p) DIM2D_LDG_HOST(p)  // host emulation with checked reads
+#else
+#define DIM2D_LDG(p) (*(p))
+#endif
+
 namespace dim2d {
 
 namespace {
@@ -38,28 +46,28 @@ struct Frame {
   Field f;
   int bx, by;  // node b (high side of the face)
   bool ydir;   // normal along y
-  __device__ __forceinline__ size_t idx(int n, int t) const {
+  __host__ __device__ __forceinline__ size_t idx(int n, int t) const {
     const int x = ydir ? bx + t : bx + n;
     const int y = ydir ? by + n : by + t;
     return (size_t)y * f.pitch + x;
   }
-  __device__ __forceinline__ Node node(int n, int t) const {
+  __host__ __device__ __forceinline__ Node node(int n, int t) const {
     const size_t o = idx(n, t);
     Node q;
-    q.r = __ldg(u + o);
-    const double mx = __ldg(u + o + f.plane), my = __ldg(u + o + 2 * f.plane);
+    q.r = DIM2D_LDG(u + o);
+    const double mx = DIM2D_LDG(u + o + f.plane), my = DIM2D_LDG(u + o + 2 * f.plane);
     q.mn = ydir ? my : mx;
     q.mt = ydir ? mx : my;
-    q.e = __ldg(u + o + 3 * f.plane);
+    q.e = DIM2D_LDG(u + o + 3 * f.plane);
     return q;
   }
-  __device__ __forceinline__ double rho(int n, int t) const { return __ldg(u + idx(n, t)); }
+  __host__ __device__ __forceinline__ double rho(int n, int t) const { return DIM2D_LDG(u + idx(n, t)); }
 };
 
 struct NP {  // primitives of a node in the frame
   double un, ut, p, tcl, cp;
 };
-__device__ __forceinline__ NP nprim(const Node& q, const DimConst& k) {
+__host__ __device__ __forceinline__ NP nprim(const Node& q, const DimConst& k) {
   const NodePrim p = node_prim(q.r, q.mn, q.mt, q.e, k);  // u <-> n, v <-> t
   NP o;
   o.un = p.u;
@@ -72,7 +80,7 @@ __device__ __forceinline__ NP nprim(const Node& q, const DimConst& k) {
 
 // Tcap at frame node (n,t): centred normal gradient, tangential gradient
 // per mode (sd_operators_fd_module.f:71-153, 182-450)
-__device__ __forceinline__ double tcap_at(const Frame& F, int n, int t, int tm, double rdn,
+__host__ __device__ __forceinline__ double tcap_at(const Frame& F, int n, int t, int tm, double rdn,
                                           double rdt) {
   const double r = F.rho(n, t);
   const double gn = 0.5 * rdn * (F.rho(n + 1, t) - F.rho(n - 1, t));
@@ -87,7 +95,7 @@ __device__ __forceinline__ double tcap_at(const Frame& F, int n, int t, int tm, 
 // with the tangential operators of mode tm (the normal operators are the
 // interior ones in every set used here: y_{L0,L1,R1,R0} change only
 // y-derivatives of x-faces, x_{...} only x-derivatives of y-faces).
-__device__ void frame_face_flux(const Frame& F, int tm, double rdn, double rdt,
+__host__ __device__ void frame_face_flux(const Frame& F, int tm, double rdn, double rdt,
                                 const DimConst& k, double out[4]) {
   const Node a = F.node(-1, 0), b = F.node(0, 0);
   const NP pa = nprim(a, k), pb = nprim(b, k);
@@ -147,7 +155,7 @@ __device__ void frame_face_flux(const Frame& F, int tm, double rdn, double rdt,
 // state of the node, g = one-sided normal gradients of (rho, u, v, P);
 // ydir = normal along y; right = E or N side.  Output: conservative
 // time derivative contribution.
-__device__ void char_term(const double q[4], const double g[4], bool ydir, bool right,
+__host__ __device__ void char_term(const double q[4], const double g[4], bool ydir, bool right,
                           const DimConst& k, double td[4]) {
   const double md = q[0];
   const double ux = q[1] / q[0], uy = q[2] / q[0];
@@ -198,17 +206,17 @@ __device__ void char_term(const double q[4], const double g[4], bool ydir, bool 
   td[3] = tp[0] * dEdrho + tp[1] * (md * ux) + tp[2] * (md * uy) + tp[3] * (k.cv_r * (1.0 - md / 3.0));
 }
 
-__device__ __forceinline__ void load4(const double* u, const Field& f, int x, int y, double q[4]) {
+__host__ __device__ __forceinline__ void load4(const double* u, const Field& f, int x, int y, double q[4]) {
   const size_t o = (size_t)y * f.pitch + x;
-  q[0] = __ldg(u + o);
-  q[1] = __ldg(u + o + f.plane);
-  q[2] = __ldg(u + o + 2 * f.plane);
-  q[3] = __ldg(u + o + 3 * f.plane);
+  q[0] = DIM2D_LDG(u + o);
+  q[1] = DIM2D_LDG(u + o + f.plane);
+  q[2] = DIM2D_LDG(u + o + 2 * f.plane);
+  q[3] = DIM2D_LDG(u + o + 3 * f.plane);
 }
 
 // one-sided normal gradient of (rho, u, v, P) at node (x,y):
 // R0 = (phi(n) - phi(n-1))/dn, L0 = (phi(n+1) - phi(n))/dn
-__device__ void prim_gradient(const double* u, const Field& f, int x, int y, bool ydir, bool right,
+__host__ __device__ void prim_gradient(const double* u, const Field& f, int x, int y, bool ydir, bool right,
                               double rdn, const DimConst& k, double g[4]) {
   const int sx = ydir ? 0 : 1, sy = ydir ? 1 : 0;
   double q0[4], q1[4];
@@ -227,16 +235,25 @@ __device__ void prim_gradient(const double* u, const Field& f, int x, int y, boo
   g[3] = rdn * (p1.p - p0.p);
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(128) k_open_ghosts(StageArgs a) {
+}  // namespace
+
+// number of ghost cells of a field open on all sides
+__host__ __device__ __forceinline__ int open_ghost_count(const Field& f) {
+  const int ex = f.nx - 2 * BC, ey = f.ny - 2 * BC;
+  return 2 * BC * ex + 2 * BC * ey + 4 * BC * BC;
+}
+
+// Ghost cell number m of a field open on all sides: time derivative
+// (mode 0) or RK stage update (mode 1) written to a.uout.  Cells are
+// numbered S edge, N edge (BC rows of ex cells each), W edge, E edge (BC
+// columns of ey cells each), then the 4 corners (SW, SE, NW, NE) of BC x BC.
+__host__ __device__ void open_ghost_cell(const StageArgs& a, int m, int mode) {
   const Field f = a.f;
   const int ex = f.nx - 2 * BC, ey = f.ny - 2 * BC;  // interior extents
-  const int n_ns = 2 * BC * ex;                       // one N or S edge
-  const int n_ew = 2 * BC * ey;
+  const int n_ns = BC * ex;                           // cells of one N or S edge
+  const int n_ew = BC * ey;                           // cells of one E or W edge
   const int n_c = BC * BC;
-  const int total = 2 * n_ns + 2 * n_ew + 4 * n_c;
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= total) return;
+  if (m < 0 || m >= open_ghost_count(f)) return;
   const DimConst& k = a.k;
   int x, y;
   double L[4];
@@ -311,18 +328,24 @@ __global__ void __launch_bounds__(128) k_open_ghosts(StageArgs a) {
 #pragma unroll
   for (int v = 0; v < 4; v++) {
     double out;
-    if (MODE == 0) out = L[v];
+    if (mode == 0) out = L[v];
     else if (a.stage == 1) out = q[v] + a.dt * L[v];
-    else out = a.b * __ldg(a.u0 + o + v * f.plane) + (1.0 - a.b) * (q[v] + a.dt * L[v]);
+    else out = a.b * DIM2D_LDG(a.u0 + o + v * f.plane) + (1.0 - a.b) * (q[v] + a.dt * L[v]);
     a.uout[o + v * f.plane] = out;
   }
+}
+
+namespace {
+
+template <int MODE>
+__global__ void __launch_bounds__(128) k_open_ghosts(StageArgs a) {
+  open_ghost_cell(a, blockIdx.x * blockDim.x + threadIdx.x, MODE);
 }
 
 }  // namespace
 
 cudaError_t launch_open_ghosts(const StageArgs& a, int mode, cudaStream_t s) {
-  const int ex = a.f.nx - 2 * BC, ey = a.f.ny - 2 * BC;
-  const int total = 4 * BC * ex + 4 * BC * ey + 4 * BC * BC;
+  const int total = open_ghost_count(a.f);
   const int blocks = (total + 127) / 128;
   if (mode == 0) k_open_ghosts<0><<<blocks, 128, 0, s>>>(a);
   else k_open_ghosts<1><<<blocks, 128, 0, s>>>(a);

@@ -37,13 +37,17 @@ def test_time_dev_all_cells(oracle, F, n, ny, seed):
     assert np.isfinite(got).all()
     err = normwise_rel_err_all(got, ref)
     assert np.all(err <= 1e-12), err
-    # ghost rows / columns / corners separately (the open-boundary kernel)
+    # ghost rows / columns / corners separately (the open-boundary kernel),
+    # normalised by the field-wide maximum like the metric above: where the
+    # boundary sees uniform flow the exact time derivative is 0 and both
+    # codes return ~1e-11 of cancellation noise, so a ghost-only norm is
+    # meaningless there
     for sl in [np.s_[:, :2, :], np.s_[:, -2:, :], np.s_[:, :, :2], np.s_[:, :, -2:]]:
         a, b = got[sl], ref[sl]
         for k in range(4):
-            den = np.abs(b[k]).max()
+            den = np.abs(ref[k]).max()
             num = np.abs(a[k] - b[k]).max()
-            assert (num / den if den > 0 else num) <= 1e-11, (sl, k)
+            assert (num / den if den > 0 else num) <= 1e-12, (sl, k)
 
 
 def test_one_step_all_cells(oracle, F):
