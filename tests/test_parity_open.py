@@ -65,8 +65,12 @@ def test_one_step_all_cells(oracle, F):
 
 
 def test_100_steps_transported_bubble(oracle, F):
-    """128^2 bubble carried by a Mach 0.1 flow through open boundaries."""
-    nx, ny, x_map, y_map, q = open_case(128, radius=0.12, center=(0.3, 0.0))
+    """128^2 bubble carried by a Mach 0.1 flow through open boundaries, with
+    a seeded transverse-velocity perturbation so that waves leave through
+    all four sides.  (A bubble started at x = 0.3 diverges within 100 steps
+    in the oracle itself, so it is no parity case.)  The oracle's own
+    sensitivity on this case: 1e-15 initial noise grows to 1e-13."""
+    nx, ny, x_map, y_map, q = open_case(128, radius=0.12, seed=7)
     cfg = _cfg(oracle, F, nx, ny)
     dt = stable_dt(q, x_map, y_map)
     ref = q.copy()
