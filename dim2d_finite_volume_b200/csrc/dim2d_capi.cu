@@ -49,6 +49,7 @@ DimConst make_const(const dim2d_params& p) {
   k.c15cv = 1.5 / p.cv_r;
   k.c3cv = 3.0 / p.cv_r;
   k.two_mu = 2.0 + p.viscous_r;
+  k.c38cv = 3.0 / (8.0 * p.cv_r);
   k.gravity_ac = p.gravity_ac;
   k.gravity = p.gravity;
   return k;
@@ -82,6 +83,36 @@ int resolve_sides(const int bc_choice[8], const int bc_type[8], int side_kind[8]
                      "periodic boundaries must be periodic on all sides (periodic_xy)");
   *periodic = nper == 8;
   return DIM2D_OK;
+}
+
+int classify_mirrors(const int bc_choice[8], const int bc_type[8], int* south_wall,
+                     int* corners_y) {
+  const int N = DIM2D_SIDE_N, S = DIM2D_SIDE_S, E = DIM2D_SIDE_E, W = DIM2D_SIDE_W;
+  if (bc_choice[N] != DIM2D_REFLECTION_Y || bc_type[N] != DIM2D_BC_NODES) return 0;
+  if (bc_choice[E] != DIM2D_REFLECTION_X || bc_type[E] != DIM2D_BC_NODES) return 0;
+  if (bc_choice[W] != DIM2D_REFLECTION_X || bc_type[W] != DIM2D_BC_NODES) return 0;
+  int wall = 0;
+  if (bc_choice[S] == DIM2D_WALL && bc_type[S] == DIM2D_BC_FLUX_AND_NODE) wall = 1;
+  else if (bc_choice[S] != DIM2D_REFLECTION_Y || bc_type[S] != DIM2D_BC_NODES) return 0;
+  const int c0 = bc_choice[DIM2D_SIDE_NE];
+  if (c0 != DIM2D_REFLECTION_X && c0 != DIM2D_REFLECTION_Y) return 0;
+  for (int s = DIM2D_SIDE_NE; s <= DIM2D_SIDE_SW; s++)
+    if (bc_choice[s] != c0 || bc_type[s] != DIM2D_BC_NODES) return 0;
+  // the wall corners mirror the wall ghost cells along x
+  if (wall && c0 != DIM2D_REFLECTION_X) return 0;
+  *south_wall = wall;
+  *corners_y = c0 == DIM2D_REFLECTION_Y;
+  return 1;
+}
+
+WallConst make_wall(const dim2d_params& p) {
+  WallConst w{};
+  w.cos_angle = std::cos(p.wall_micro_contact_angle * std::acos(-1.0) / 180.0);
+  w.heat_choice = p.wall_heat_source_choice;
+  w.qmax = p.wall_maximum_heat_flux;
+  w.qcenter = p.wall_heat_source_center;
+  w.qvariance = p.wall_heat_source_variance;
+  return w;
 }
 
 int all_open(const int bc_choice[8], const int bc_type[8]) {
@@ -147,10 +178,16 @@ int dim2d_create(const dim2d_params* p, int nx, int ny, const int bc_choice[8],
   int rc = resolve_sides(bc_choice, bc_type, side_kind, &periodic);
   if (rc) return rc;
   const int open = all_open(bc_choice, bc_type);
-  if (!periodic && !open)
+  int south_wall = 0, corners_y = 0;
+  const int mirrors = !periodic && !open && classify_mirrors(bc_choice, bc_type, &south_wall,
+                                                             &corners_y);
+  if (!periodic && !open && !mirrors)
     return set_error(DIM2D_ERR_UNSUPPORTED,
-                     "create: boundary configuration not provided (periodic_xy and hedstrom_xy "
-                     "are)");
+                     "create: boundary configuration not provided (periodic_xy, hedstrom_xy, "
+                     "reflection_xy and wall_S_reflection are)");
+  if (south_wall && p->wall_heat_source_choice != 0 && !(p->wall_heat_source_variance > 0) &&
+      p->wall_heat_source_choice == 2)
+    return set_error(DIM2D_ERR_ARG, "create: gaussian heat source needs a positive variance");
   if (precision != DIM2D_FP64)
     return set_error(DIM2D_ERR_UNSUPPORTED, "create: mixed precision not provided by this build");
 
@@ -160,6 +197,10 @@ int dim2d_create(const dim2d_params* p, int nx, int ny, const int bc_choice[8],
   h->precision = precision;
   h->periodic = periodic;
   h->open_all = open;
+  h->mirrors = mirrors;
+  h->south_wall = south_wall;
+  h->corners_y = corners_y;
+  h->wall = make_wall(*p);
   std::memcpy(h->bc_choice, bc_choice, sizeof h->bc_choice);
   std::memcpy(h->bc_type, bc_type, sizeof h->bc_type);
   std::memcpy(h->bc_order, bc_order, sizeof h->bc_order);
@@ -187,6 +228,7 @@ int dim2d_create(const dim2d_params* p, int nx, int ny, const int bc_choice[8],
   e = cudaMalloc(&h->x_map, nx * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&h->y_map, ny * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&h->scalar, 4 * sizeof(double));
+  if (e == cudaSuccess) h->status = reinterpret_cast<unsigned int*>(h->scalar + 2);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -196,6 +238,7 @@ int dim2d_create(const dim2d_params* p, int nx, int ny, const int bc_choice[8],
   h->stream = h->own_stream;
   // keep never-written pitch padding and ghost cells defined
   for (double* b : {h->A, h->B, h->C}) cudaMemsetAsync(b, 0, bytes, h->stream);
+  cudaMemsetAsync(h->scalar, 0, 4 * sizeof(double), h->stream);
   *out = h;
   return DIM2D_OK;
 }
@@ -250,6 +293,8 @@ int dim2d_upload(dim2d_handle* h, const double* nodes, const double* x_map, cons
   if (!(h->dx > 0) || !(h->dy > 0)) return set_error(DIM2D_ERR_ARG, "upload: x_map/y_map not increasing");
   h->rdx = 1.0 / h->dx;
   h->rdy = 1.0 / h->dy;
+  h->xmap0 = x_map[0];
+  h->ymap0 = y_map[0];
   h->x_min = x_map[BC];
   h->x_max = x_map[f.nx - 1 - BC];
   h->y_min = y_map[BC];
@@ -321,20 +366,13 @@ int dim2d_time_dev(dim2d_handle* h, double* time_dev) {
   // td_operators_class.f:150-154: every cell starts at debug_real
   e = launch_fill(h->td, 9.9692099683868690e+36, 4 * f.plane, h->stream);
   h->launches++;
+  const StageArgs a = make_stage_args(h, h->A, h->td, 0.0, 0);
   if (e == cudaSuccess) {
-    e = launch_time_dev(h->A, h->td, f, h->rdx, h->rdy, h->k, h->stream);
+    e = launch_time_dev(a, h->stream);
     h->launches++;
   }
   if (e == cudaSuccess && h->open_all) {
     // bc_operators_hedstrom_xy_class.f:182-496: ghost-cell time derivatives
-    StageArgs a{};
-    a.uin = h->A;
-    a.u0 = h->A;
-    a.uout = h->td;
-    a.f = f;
-    a.rdx = h->rdx;
-    a.rdy = h->rdy;
-    a.k = h->k;
     e = launch_open_ghosts(a, 0, h->stream);
     h->launches++;
   }

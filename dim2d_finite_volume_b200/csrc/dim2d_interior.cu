@@ -37,7 +37,7 @@ constexpr int SM_FY = 4 * (TY + 1) * TX;
 constexpr int SM_DOUBLES = SM_RAW + SM_PRIM + SM_FX + SM_FY;
 
 // mode: 0 = write L(u) (time derivative), 1 = RK stage update
-template <int MODE>
+template <int MODE, bool WALL>
 __global__ void __launch_bounds__(NT, 2) k_interior(StageArgs a) {
   extern __shared__ __align__(16) double sm[];
   double* sR = sm;
@@ -127,7 +127,19 @@ __global__ void __launch_bounds__(NT, 2) k_interior(StageArgs a) {
       fi.lap = d2n + d2t;
       fi.dtn = rdx * (fi.tb - fi.ta);
       fi.dkn = rdx * (fi.kb - fi.ka);
-      face_flux(fi, k, F);
+      const int gxf = x0 + fx;  // face between columns gxf-1 and gxf
+      const bool w_face = WALL && a.wall_w && gxf == BC;
+      const bool e_face = WALL && a.wall_e && gxf == f.nx - BC;
+      if (w_face || e_face) {
+        // bc_operators_wall_xy_class.f:751-771: wall x-face; the low
+        // temperature is taken on the interior side (:473-490)
+        const int p = w_face ? pR : pL;
+        const double tl = k.c38cv * (sT[p] - k.iwe * sK[p]);
+        const double q = wall_heat_flux(a.wall, a.xmap0 + gxf * a.dx);
+        wall_face_flux(fi, tl, a.dx, q, w_face ? q : -q, k, F);
+      } else {
+        face_flux(fi, k, F);
+      }
       const int o = fy * (TX + 1) + fx;
       sFx[o] = F[0];
       sFx[o + TY * (TX + 1)] = F[1];
@@ -161,7 +173,18 @@ __global__ void __launch_bounds__(NT, 2) k_interior(StageArgs a) {
       fi.lap = d2n + d2t;
       fi.dtn = rdy * (fi.tb - fi.ta);
       fi.dkn = rdy * (fi.kb - fi.ka);
-      face_flux(fi, k, F);
+      const int gyf = y0 + gy;  // face between rows gyf-1 and gyf
+      const bool s_face = WALL && a.wall_s && gyf == BC;
+      const bool n_face = WALL && a.wall_n && gyf == f.ny - BC;
+      if (s_face || n_face) {
+        // bc_operators_wall_xy_class.f:729-749: wall y-face (:818-852)
+        const int p = s_face ? pT : pB;
+        const double tl = k.c38cv * (sT[p] - k.iwe * sK[p]);
+        const double q = wall_heat_flux(a.wall, a.xmap0 + (x0 + gx) * a.dx);
+        wall_face_flux(fi, tl, a.dy, q, s_face ? q : -q, k, F);
+      } else {
+        face_flux(fi, k, F);
+      }
       const int o = gy * TX + gx;
       sFy[o] = F[0];
       sFy[o + (TY + 1) * TX] = F[2];      // momentum_x is tangential on a y-face
@@ -268,43 +291,41 @@ __global__ void k_cfl_max(const double* __restrict__ u, Field f, DimConst k,
 
 size_t interior_smem_bytes() { return SM_DOUBLES * sizeof(double); }
 
+// The dynamic shared-memory opt-in is a per-device function attribute.
 static cudaError_t set_smem_attr() {
-  static bool done = false;
-  if (done) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(k_interior<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)interior_smem_bytes());
+  static bool done[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_interior<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)interior_smem_bytes());
-  if (e != cudaSuccess) return e;
-  done = true;
+  if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+  const int bytes = (int)interior_smem_bytes();
+  const void* fns[4] = {(const void*)k_interior<0, false>, (const void*)k_interior<1, false>,
+                        (const void*)k_interior<0, true>, (const void*)k_interior<1, true>};
+  for (const void* fn : fns) {
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+  }
+  if (dev >= 0 && dev < 64) done[dev] = true;
   return cudaSuccess;
 }
 
-cudaError_t launch_interior_stage(const StageArgs& a, cudaStream_t s) {
+template <int MODE>
+static cudaError_t launch_mode(const StageArgs& a, cudaStream_t s) {
   cudaError_t e = set_smem_attr();
   if (e != cudaSuccess) return e;
   dim3 grid((a.f.nx - 2 * BC + TX - 1) / TX, (a.f.ny - 2 * BC + TY - 1) / TY);
-  k_interior<1><<<grid, NT, interior_smem_bytes(), s>>>(a);
+  if (a.wall_w || a.wall_e || a.wall_s || a.wall_n)
+    k_interior<MODE, true><<<grid, NT, interior_smem_bytes(), s>>>(a);
+  else
+    k_interior<MODE, false><<<grid, NT, interior_smem_bytes(), s>>>(a);
   return cudaGetLastError();
 }
 
-cudaError_t launch_time_dev(const double* uin, double* td, const Field& f, double rdx, double rdy,
-                            const DimConst& k, cudaStream_t s) {
-  cudaError_t e = set_smem_attr();
-  if (e != cudaSuccess) return e;
-  StageArgs a{};
-  a.uin = uin;
-  a.u0 = uin;
-  a.uout = td;
-  a.f = f;
-  a.rdx = rdx;
-  a.rdy = rdy;
-  a.k = k;
-  dim3 grid((f.nx - 2 * BC + TX - 1) / TX, (f.ny - 2 * BC + TY - 1) / TY);
-  k_interior<0><<<grid, NT, interior_smem_bytes(), s>>>(a);
-  return cudaGetLastError();
+cudaError_t launch_interior_stage(const StageArgs& a, cudaStream_t s) {
+  return launch_mode<1>(a, s);
 }
+
+cudaError_t launch_time_dev(const StageArgs& a, cudaStream_t s) { return launch_mode<0>(a, s); }
 
 cudaError_t launch_fill(double* p, double v, size_t n, cudaStream_t s) {
   int blocks = (int)((n + 255) / 256);

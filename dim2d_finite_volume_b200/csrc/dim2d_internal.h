@@ -15,6 +15,12 @@ struct dim2d_handle {
   int precision = 0;
   int periodic = 0;
   int open_all = 0;  // hedstrom_xy: every section open, type bc_timedev
+  int mirrors = 0;     // reflection_xy or wall_S_reflection (node pass kernel)
+  int south_wall = 0;  // wall_S_reflection
+  int corners_y = 0;   // corner sections are reflection_y
+  dim2d::WallConst wall{};
+  unsigned int* status = nullptr;  // wall root status word (device)
+  double xmap0 = 0, ymap0 = 0;     // x_map(1), y_map(1)
   int bc_choice[8]{}, bc_type[8]{}, bc_order[8]{};
   int side_kind[8]{};
   dim2d::Field f{};
@@ -52,7 +58,18 @@ int resolve_sides(const int bc_choice[8], const int bc_type[8], int side_kind[8]
 int all_open(const int bc_choice[8], const int bc_type[8]);
 }  // namespace dim2d
 
+// Mirror / south-wall configurations (library_config.py:58-115): returns 1
+// and sets the flags when bc_choice/bc_type are reflection_xy or
+// wall_S_reflection.
+namespace dim2d {
+int classify_mirrors(const int bc_choice[8], const int bc_type[8], int* south_wall,
+                     int* corners_y);
+WallConst make_wall(const dim2d_params& p);
+}  // namespace dim2d
+
 // dim2d_step.cu
+dim2d::StageArgs make_stage_args(const dim2d_handle* h, const double* uin, double* uout,
+                                 double dt, int st);
 int rk3_step(dim2d_handle* h, double dt);
 int apply_bc_on_nodes(dim2d_handle* h, const double* nodes_tmp, double* nodes);
 int check_status(dim2d_handle* h);

@@ -18,6 +18,22 @@ struct Field {
 // Boundary layout of a field, resolved on the host from bc_choice/bc_type.
 enum SideKind : int { SIDE_PERIODIC = 0, SIDE_WALL = 1, SIDE_OPEN = 2, SIDE_REFLECT = 3 };
 
+// Wall constants (parameters_input.f:526-624): uniform micro contact angle
+// (its cosine precomputed on the host, wall_xy_equilibrium_module.f:2262)
+// and the wall heat source (no / constant / gaussian, :1645-1707).
+struct WallConst {
+  double cos_angle;
+  int heat_choice;  // 0 none, 1 constant, 2 gaussian
+  double qmax, qcenter, qvariance;
+};
+
+__host__ __device__ __forceinline__ double wall_heat_flux(const WallConst& w, double x) {
+  if (w.heat_choice == 0) return 0.0;
+  if (w.heat_choice == 1) return w.qmax;
+  const double z = (x - w.qcenter) / w.qvariance;
+  return w.qmax * exp(-0.5 * (z * z));
+}
+
 struct StageArgs {
   const double* __restrict__ uin;  // state the stencil reads
   const double* __restrict__ u0;   // u^n (stages 2 and 3)
@@ -29,8 +45,27 @@ struct StageArgs {
   int stage;                       // 1, 2, 3
   int periodic;                    // write periodic ghost images of edge cells
   int wall_w, wall_e, wall_s, wall_n;  // wall flux override on that side
+  double t;                            // field time (constant over the stages)
+  double xmap0, ymap0;                 // x_map(1), y_map(1): x_map(i) = xmap0 + (i-1) dx
+  WallConst wall;
   DimConst k;
 };
+
+// Node boundary pass of a field whose sides are mirrors (reflection_x/_y)
+// or, on the south side, the wall operator.
+struct NodeBcArgs {
+  const double* __restrict__ utmp;  // nodes_tmp = u^n (wall temperature guess)
+  double* __restrict__ u;           // field whose ghosts are set
+  Field f;
+  double dx, dy, rdx, rdy;
+  double t, xmap0, ymap0;
+  int south_wall;                   // 1: wall on S (wall_S_reflection), 0: mirror
+  int corners_y;                    // corners are reflection_y (reflection_xy) vs _x
+  unsigned int* status;             // bit 0: root not bracketed, bits 1-3: Ridders
+  WallConst wall;
+  DimConst k;
+};
+cudaError_t launch_node_bc(const NodeBcArgs& a, cudaStream_t s);
 
 // Tile of the fused interior kernel: TX x TY interior cells per CTA.
 constexpr int TILE_X = 32;
@@ -38,8 +73,8 @@ constexpr int TILE_Y = 8;
 size_t interior_smem_bytes();
 
 cudaError_t launch_interior_stage(const StageArgs& a, cudaStream_t s);
-cudaError_t launch_time_dev(const double* uin, double* td, const Field& f, double rdx, double rdy,
-                            const DimConst& k, cudaStream_t s);
+// L(a.uin) of the interior cells into a.uout (stage fields ignored)
+cudaError_t launch_time_dev(const StageArgs& a, cudaStream_t s);
 // open (Hedstrom) ghost cells of a field open on all sides; mode 0 writes
 // L(u) into a.uout, mode 1 the RK stage update
 cudaError_t launch_open_ghosts(const StageArgs& a, int mode, cudaStream_t s);

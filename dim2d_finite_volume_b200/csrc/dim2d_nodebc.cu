@@ -1,0 +1,304 @@
+// dim2d_nodebc.cu -- node boundary pass for mirror sides and the south
+// wall on sm_100a.
+//
+// Configurations (the reference's presets, library_config.py:58-115):
+//   reflection_xy      N/S reflection_y, E/W reflection_x, corners reflection_y
+//   wall_S_reflection  S wall, N reflection_y, E/W reflection_x, corners reflection_x
+// Mirrors: bc_operators_reflection_{x,y}_class.f:178-296 (prefactor -1 on
+// the normal momentum, reflection_xy_module.f:50-110).  Every mirror ghost
+// is a signed copy of an interior node, so all of them are computed
+// straight from the interior, in one launch, whatever the section order.
+// The corners of wall_S_reflection on the south side mirror the wall ghost
+// cells; the thread that solves a wall column writes them too.
+//
+// Wall ghost cell (wall_xy_equilibrium_module.f:948-1040, 1747-2461):
+// density of the first ghost row = root in [rho_vap(T), rho_liq(T)] of the
+// contact-angle equilibrium function (bracket scan of at most 99 steps,
+// then Ridders' method with at most 60 iterations, xacc = 1e-12,
+// ridders_method_module.f:112-216); second ghost row by extrapolation;
+// ghost momenta from the first interior velocity.  Where the reference
+// stops the program (no bracket, no convergence) the kernel writes NaN and
+// sets a bit of the status word the host reads after the step.
+#include "dim2d_kernels.cuh"
+
+#ifdef __CUDA_ARCH__
+#define NBC_LDG(p) __ldg(p)
+#define NBC_ST(p, v) (*(p) = (v))
+#elif defined(DIM2D_LDG_HOST)
+#define NBC_LDG(p) DIM2D_LDG_HOST(p)  // host emulation: checked reads and writes
+#define NBC_ST(p, v) DIM2D_ST_HOST(p, v)
+#else
+#define NBC_LDG(p) (*(p))
+#define NBC_ST(p, v) (*(p) = (v))
+#endif
+
+namespace dim2d {
+
+namespace {
+
+__host__ __device__ __forceinline__ int mirror_lo_hi(int i, int n) {
+  // ghost index -> mirrored interior index (bc_size = 2)
+  return i < BC ? 2 * BC - 1 - i : 2 * n - 2 * BC - 1 - i;
+}
+
+// wall root function context (wall_x_root_fct, :2016-2103)
+struct WallRoot {
+  double md1;  // md_x(2): first interior density
+  double md2;  // md_x(1): second interior density
+  double my0, my1;
+  double vx, vy, Ed;
+  double dxn, dyt;  // delta_x (normal), delta_y (tangential)
+  double q;
+  double cosang;
+};
+
+// dim2d_state_eq_module.f:56-227 (high-temperature fits)
+__host__ __device__ __forceinline__ double md_vap(double T) { return 1.0 - 1.91 * sqrt(1.0 - T); }
+__host__ __device__ __forceinline__ double md_liq(double T) { return 1.0 + 2.06 * sqrt(1.0 - T); }
+
+// wall_x_equilibrium_root_fct(md_x(2), [md_x(1), x], ...), :2151-2212
+__host__ __device__ double wall_root_f(const WallRoot& c, double x, const DimConst& k) {
+  const double dmddx_half = (-c.md1 + x) / (c.dxn);
+  const double md_av = 0.5 * (c.md1 + x);
+  const double gx = (x - c.md2) / (2.0 * c.dxn);        // dmddx, interior type
+  const double gy = (c.my1 - c.my0) / (2.0 * c.dyt);    // dmddx, interior type
+  const double g2 = gx * gx + gy * gy;
+  const double T1 = 3.0 / (8.0 * k.cv_r) *
+                    (c.Ed / c.md1 - 0.5 * (c.vx * c.vx + c.vy * c.vy) -
+                     0.5 / k.we * g2 / c.md1 + 3.0 * c.md1);           // :2382-2407
+  const double Tav = T1 + 0.5 * c.dxn * k.re * k.pr * 3.0 / (8.0 * k.cv_r) * c.q;  // :2295-2315
+  const double mv = md_vap(Tav), ml = md_liq(Tav);
+  const double s = sqrt(1.0 - Tav);
+  const double st = 2.0 * sqrt(2.0) / (3.0 * sqrt(k.we)) * (9.691686257306483 * (s * s * s));
+  const double d = ml - mv;
+  const double dE = 6.0 * (md_av - ml) * (md_av - mv) / (d * d * d) * st * c.cosang;  // :2238-2270
+  return 1.0 / k.we * dmddx_half + dE;
+}
+
+__host__ __device__ __forceinline__ bool same_sign(double a, double b) {
+  return copysign(1.0, a) * copysign(1.0, b) > 0;  // :1962-1972
+}
+__host__ __device__ __forceinline__ bool validated(double a, double b) { return fabs(a - b) < 1e-10; }
+
+// :1846-1941 then ridders_method_module.f:112-216.  Returns the root;
+// *status gets 1 (no bracket), 2 (not bracketed), 3 (no convergence) or
+// 4 (bracketing error).
+__host__ __device__ double wall_root(const WallRoot& c, double T_guess, double md_guess,
+                                     const DimConst& k, unsigned int* status) {
+  double xl = md_vap(T_guess), xh = md_liq(T_guess);
+  double fl = wall_root_f(c, xl, k), fh = wall_root_f(c, xh, k);
+  if (same_sign(fl, fh)) {
+    const double dmd_l = md_guess / 100.0, dmd_r = (3.0 - md_guess) / 100.0;
+    const double fmd = wall_root_f(c, md_guess, k);
+    bool found = false;
+    for (int j = 1; j <= 99 && !found; j++) {
+      const double a = md_guess - j * dmd_l, b = md_guess + j * dmd_r;
+      const double fa = wall_root_f(c, a, k), fb = wall_root_f(c, b, k);
+      if (!same_sign(fa, fmd)) {
+        xl = a;
+        xh = md_guess;
+        found = true;
+      } else if (!same_sign(fb, fmd)) {
+        xl = md_guess;
+        xh = b;
+        found = true;
+      }
+    }
+    if (!found) {
+      *status |= 1u;
+      return NAN;
+    }
+  }
+  // Ridders' method
+  const double xacc = 1e-12;
+  const double UNUSED = (double)(-1.11e30f);
+  fl = wall_root_f(c, xl, k);
+  fh = wall_root_f(c, xh, k);
+  double x = UNUSED;
+  if ((fl > 0.0 && fh < 0.0) || (fl < 0.0 && fh > 0.0)) {
+    const double x1 = xl;
+    (void)x1;
+    for (int j = 1; j <= 60; j++) {
+      const double xm = 0.5 * (xl + xh);
+      const double fm = wall_root_f(c, xm, k);
+      const double s = sqrt(fm * fm - fl * fh);
+      if (validated(s, 0.0)) return x;
+      const double xnew = xm + (xm - xl) * (copysign(1.0, fl - fh) * fm / s);
+      if (fabs(xnew - x) <= xacc) return x;
+      x = xnew;
+      const double fnew = wall_root_f(c, x, k);
+      if (validated(fnew, 0.0)) return x;
+      if (!validated(copysign(fm, fnew), fm)) {
+        xl = xm;
+        fl = fm;
+        xh = x;
+        fh = fnew;
+      } else if (!validated(copysign(fl, fnew), fl)) {
+        xh = x;
+        fh = fnew;
+      } else if (!validated(copysign(fh, fnew), fh)) {
+        xl = x;
+        fl = fnew;
+      } else {
+        *status |= 8u;
+        return x;
+      }
+      if (fabs(xh - xl) <= xacc) return x;
+    }
+    *status |= 4u;
+    return x;
+  }
+  if (validated(fl, 0.0)) return xl;
+  if (validated(fh, 0.0)) return xh;
+  *status |= 2u;
+  return x;
+}
+
+__host__ __device__ __forceinline__ double ld(const double* p, const Field& f, int v, int x, int y) {
+  return NBC_LDG(p + (size_t)v * f.plane + (size_t)y * f.pitch + x);
+}
+
+}  // namespace
+
+__host__ __device__ int node_bc_count(const NodeBcArgs& a) {
+  const int ex = a.f.nx - 2 * BC, ey = a.f.ny - 2 * BC;
+  const int n_we = 2 * BC * ey, n_n = BC * ex, n_s = a.south_wall ? ex : BC * ex;
+  const int n_c = (a.south_wall ? 2 : 4) * BC * BC;
+  return n_we + n_n + n_s + n_c;
+}
+
+// Ghost work item m: W/E mirror cells, N mirror cells, S cells (wall
+// columns or mirror cells), then corner cells.
+__host__ __device__ void node_bc_cell(const NodeBcArgs& a, int m) {
+  const Field f = a.f;
+  const int nx = f.nx, ny = f.ny;
+  const int ex = nx - 2 * BC, ey = ny - 2 * BC;
+  const int n_we = 2 * BC * ey, n_n = BC * ex, n_s = a.south_wall ? ex : BC * ex;
+  if (m < 0 || m >= node_bc_count(a)) return;
+  const double pre_x[4] = {1.0, -1.0, 1.0, 1.0};
+  const double pre_y[4] = {1.0, 1.0, -1.0, 1.0};
+  double* u = a.u;
+  if (m < n_we) {  // reflection_x, bc_operators_reflection_x_class.f:212-234
+    const bool east = m >= BC * ey;
+    const int r = east ? m - BC * ey : m;
+    const int y = BC + r % ey;
+    const int col = r / ey;
+    const int x = east ? nx - BC + col : col;
+    const int sx = mirror_lo_hi(x, nx);
+    for (int v = 0; v < 4; v++)
+      NBC_ST(&u[(size_t)v * f.plane + (size_t)y * f.pitch + x], pre_x[v] * ld(u, f, v, sx, y));
+    return;
+  }
+  m -= n_we;
+  if (m < n_n) {  // reflection_y, bc_operators_reflection_y_class.f:211-221
+    const int x = BC + m % ex;
+    const int y = ny - BC + m / ex;
+    const int sy = mirror_lo_hi(y, ny);
+    for (int v = 0; v < 4; v++)
+      NBC_ST(&u[(size_t)v * f.plane + (size_t)y * f.pitch + x], pre_y[v] * ld(u, f, v, x, sy));
+    return;
+  }
+  m -= n_n;
+  if (m < n_s) {
+    if (!a.south_wall) {  // reflection_y, :223-233
+      const int x = BC + m % ex;
+      const int y = m / ex;
+      const int sy = mirror_lo_hi(y, ny);
+      for (int v = 0; v < 4; v++)
+        NBC_ST(&u[(size_t)v * f.plane + (size_t)y * f.pitch + x], pre_y[v] * ld(u, f, v, x, sy));
+      return;
+    }
+    // wall ghost column x: ghost rows 1 (first) and 0 (second),
+    // interior rows 2 (first) and 3 (second)
+    const int x = BC + m;
+    const DimConst& k = a.k;
+    // temperature guess from u^n at the first interior node
+    // (bc_operators_wall_xy_class.f:898-930, temperature_eff
+    // dim2d_prim_module.f:652-691 with centred gradients)
+    double Tg;
+    {
+      const double r = ld(a.utmp, f, 0, x, 2);
+      const double mx = ld(a.utmp, f, 1, x, 2), my = ld(a.utmp, f, 2, x, 2);
+      const double E = ld(a.utmp, f, 3, x, 2);
+      const double gx = 0.5 / a.dx * (-ld(a.utmp, f, 0, x - 1, 2) + ld(a.utmp, f, 0, x + 1, 2));
+      const double gy = 0.5 / a.dy * (-ld(a.utmp, f, 0, x, 1) + ld(a.utmp, f, 0, x, 3));
+      const double vx = mx / r, vy = my / r;
+      const double teff = 1.0 / r * (E - 0.5 * r * (vx * vx + vy * vy) -
+                                     0.5 / k.we * (gx * gx + gy * gy) + 3.0 * (r * r));
+      Tg = 3.0 / (8.0 * k.cv_r) * teff;
+    }
+    const double md_guess = ld(a.utmp, f, 0, x, 1);
+    // compute_wall_S_ghost_cell, wall_xy_equilibrium_module.f:948-1040
+    const double r1 = ld(u, f, 0, x, 2), r2 = ld(u, f, 0, x, 3);
+    const double mx1 = ld(u, f, 1, x, 2), my1 = ld(u, f, 2, x, 2);
+    WallRoot c;
+    c.md1 = r1;
+    c.md2 = r2;
+    // md_y: neighbours of the first interior node; the W/E ghosts at the
+    // ends are mirrors (applied before S in the preset's order)
+    c.my0 = x - 1 < BC ? ld(u, f, 0, mirror_lo_hi(x - 1, nx), 2) : ld(u, f, 0, x - 1, 2);
+    c.my1 = x + 1 >= nx - BC ? ld(u, f, 0, mirror_lo_hi(x + 1, nx), 2) : ld(u, f, 0, x + 1, 2);
+    c.vx = -my1 / r1;
+    c.vy = mx1 / r1;
+    c.Ed = ld(u, f, 3, x, 2);
+    c.dxn = a.dy;
+    c.dyt = a.dx;
+    c.q = wall_heat_flux(a.wall, a.xmap0 + x * a.dx);
+    c.cosang = a.wall.cos_angle;
+    unsigned int st = 0;
+    const double rg = wall_root(c, Tg, md_guess, k, &st);
+    if (st && a.status) {
+#ifdef __CUDA_ARCH__
+      atomicOr(a.status, st);
+#else
+      *a.status |= st;
+#endif
+    }
+    const double rg2 = r2 + 3.0 * (-r1 + rg);      // :1439-1465 (high-order extrapolation)
+    const double mxg = -1.0 * mx1 / r1 * rg;        // sign_trans
+    const double myg = 1.0 * my1 / r1 * rg;         // sign_normal
+    NBC_ST(&u[(size_t)1 * f.pitch + x], rg);
+    NBC_ST(&u[(size_t)0 * f.pitch + x], rg2);
+    NBC_ST(&u[f.plane + (size_t)1 * f.pitch + x], mxg);
+    NBC_ST(&u[2 * f.plane + (size_t)1 * f.pitch + x], myg);
+    // south corners (reflection_x of these ghost cells,
+    // bc_operators_reflection_x_class.f:236-286)
+    int cx = -1;
+    if (x < 2 * BC) cx = 2 * BC - 1 - x;
+    else if (x >= nx - 2 * BC) cx = 2 * nx - 2 * BC - 1 - x;
+    if (cx >= 0) {
+      NBC_ST(&u[(size_t)1 * f.pitch + cx], pre_x[0] * rg);
+      NBC_ST(&u[(size_t)0 * f.pitch + cx], pre_x[0] * rg2);
+      NBC_ST(&u[f.plane + (size_t)1 * f.pitch + cx], pre_x[1] * mxg);
+      NBC_ST(&u[2 * f.plane + (size_t)1 * f.pitch + cx], pre_x[2] * myg);
+    }
+    return;
+  }
+  m -= n_s;
+  {  // corners from the interior: pre_x * pre_y * u(mirror x, mirror y)
+    const int nc = BC * BC;
+    int c = m / nc;
+    const int r = m % nc;
+    if (a.south_wall) c += 2;  // only NW (2) and NE (3)
+    const bool east = c & 1, north = c >> 1;
+    const int x = (east ? nx - BC : 0) + r % BC;
+    const int y = (north ? ny - BC : 0) + r / BC;
+    const int sx = mirror_lo_hi(x, nx), sy = mirror_lo_hi(y, ny);
+    for (int v = 0; v < 4; v++)
+      NBC_ST(&u[(size_t)v * f.plane + (size_t)y * f.pitch + x], pre_x[v] * pre_y[v] * ld(u, f, v, sx, sy));
+  }
+}
+
+namespace {
+__global__ void __launch_bounds__(128) k_node_bc(NodeBcArgs a) {
+  node_bc_cell(a, blockIdx.x * blockDim.x + threadIdx.x);
+}
+}  // namespace
+
+cudaError_t launch_node_bc(const NodeBcArgs& a, cudaStream_t s) {
+  const int n = node_bc_count(a);
+  k_node_bc<<<(n + 127) / 128, 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace dim2d

@@ -28,6 +28,7 @@ struct DimConst {
   double c15cv;      // 1.5/cv_r    (dim2d_fluxes_module.f:691)
   double c3cv;       // 3/cv_r      (dim2d_prim_module.f:433)
   double two_mu;     // 2+viscous_r (dim2d_fluxes_module.f:636)
+  double c38cv;      // 3/(8 cv_r): temperature from Tcl (wall_xy_equilibrium_module.f:476)
   int gravity_ac;
   double gravity;
 };
@@ -126,6 +127,25 @@ __host__ __device__ __forceinline__ void face_flux(const FaceIn& f, const DimCon
                        avr * f.drn * (f.dunn + f.dutt) - k.irepr * f.dkn;
     out[3] = inv - k.ire * vis - k.iwe * cap;
   }
+}
+
+// Flux through a wall face, in the face frame (out = {mass, momentum_n,
+// momentum_t, energy}); wall_xy_equilibrium_module.f:249-402 with
+// :445-908.  tl = 3/(8 cv_r) temperature_eff at the interior-side node;
+// dn = grid step along the normal; q = wall heat flux; q_out = +q on the
+// low (S/W) side, -q on the high (N/E) side.
+__host__ __device__ __forceinline__ void wall_face_flux(const FaceIn& f, double tl, double dn,
+                                                        double q, double q_out,
+                                                        const DimConst& k, double out[4]) {
+  const double th = tl + dn * k.c38cv * k.re * k.pr * q;
+  const double t_half = 0.5 * (tl + th);
+  const double md_half = 0.5 * (f.ra + f.rb);
+  // dim2d_prim_module.f:476-488
+  const double p = 8.0 * md_half * t_half / (3.0 - md_half) - 3.0 * (md_half * md_half);
+  out[0] = 0.0;
+  out[1] = p - k.iwe * (md_half * f.lap + 0.5 * (-(f.drn * f.drn) + (f.drt * f.drt)));
+  out[2] = -k.ire * f.dutn - k.iwe * (-f.drn * f.drt);
+  out[3] = q_out;
 }
 
 // Speed of sound, dim2d_prim_module.f:1179-1215.

@@ -6,23 +6,71 @@
 // then A and B swap.  u^n stays intact in A until the last boundary pass,
 // which the wall operator reads as nodes_tmp (bc_operators_wall_xy_class.f).
 // Each stage is followed by the node boundary pass; for periodic fields the
-// stage kernel writes the ghost images itself.
+// stage kernel writes the ghost images itself, for open fields a second
+// kernel integrates the ghost cells.
 #include <utility>
 
 #include "dim2d_internal.h"
 
 using namespace dim2d;
 
+StageArgs make_stage_args(const dim2d_handle* h, const double* uin, double* uout, double dt,
+                          int st) {
+  StageArgs a{};
+  a.uin = uin;
+  a.u0 = h->A;
+  a.uout = uout;
+  a.f = h->f;
+  a.dx = h->dx;
+  a.dy = h->dy;
+  a.rdx = h->rdx;
+  a.rdy = h->rdy;
+  a.dt = dt;
+  a.stage = st;
+  a.b = st == 2 ? 0.75 : (st == 3 ? 1.0 / 3.0 : 0.0);  // rk3tvd_steps_module.f:225,444
+  a.periodic = h->periodic;
+  a.wall_s = h->south_wall;
+  a.t = h->t;
+  a.xmap0 = h->xmap0;
+  a.ymap0 = h->ymap0;
+  a.wall = h->wall;
+  a.k = h->k;
+  return a;
+}
+
+static NodeBcArgs make_node_args(const dim2d_handle* h, const double* utmp, double* u) {
+  NodeBcArgs a{};
+  a.utmp = utmp;
+  a.u = u;
+  a.f = h->f;
+  a.dx = h->dx;
+  a.dy = h->dy;
+  a.rdx = h->rdx;
+  a.rdy = h->rdy;
+  a.t = h->t;
+  a.xmap0 = h->xmap0;
+  a.ymap0 = h->ymap0;
+  a.south_wall = h->south_wall;
+  a.corners_y = h->corners_y;
+  a.status = h->status;
+  a.wall = h->wall;
+  a.k = h->k;
+  return a;
+}
+
 int apply_bc_on_nodes(dim2d_handle* h, const double* nodes_tmp, double* nodes) {
-  (void)nodes_tmp;
+  cudaError_t e = cudaSuccess;
   if (h->periodic) {
-    cudaError_t e = launch_periodic_ghosts(nodes, h->f, h->stream);
+    e = launch_periodic_ghosts(nodes, h->f, h->stream);
     h->launches++;
-    if (e != cudaSuccess) return cuda_error(e, "apply_bc_on_nodes(periodic)");
-    return DIM2D_OK;
+  } else if (h->open_all) {
+    return DIM2D_OK;  // no section of node type
+  } else {
+    e = launch_node_bc(make_node_args(h, nodes_tmp, nodes), h->stream);
+    h->launches++;
   }
-  if (h->open_all) return DIM2D_OK;  // no section of node type
-  return set_error(DIM2D_ERR_UNSUPPORTED, "apply_bc_on_nodes: configuration not provided");
+  if (e != cudaSuccess) return cuda_error(e, "apply_bc_on_nodes");
+  return DIM2D_OK;
 }
 
 void prof_begin(dim2d_handle* h) {
@@ -46,26 +94,23 @@ void prof_end(dim2d_handle* h) {
   h->prof_used += 2;
 }
 
+// Read the wall status word (synchronising).  Non-zero = a wall ghost cell
+// had no bracketed / converged root, where the reference stops.
 int check_status(dim2d_handle* h) {
-  (void)h;
+  if (!h->south_wall || !h->status) return DIM2D_OK;
+  unsigned int st = 0;
+  cudaError_t e = cudaMemcpyAsync(&st, h->status, sizeof st, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_error(e, "status");
+  if (st)
+    return set_error(DIM2D_ERR_WALL_ROOT,
+                     "wall ghost cell: %s (status 0x%x)",
+                     (st & 1u) ? "root not bracketed" : "Ridders' method did not converge", st);
   return DIM2D_OK;
 }
 
 static int stage(dim2d_handle* h, int st, const double* uin, double* uout, double dt) {
-  StageArgs a{};
-  a.uin = uin;
-  a.u0 = h->A;
-  a.uout = uout;
-  a.f = h->f;
-  a.dx = h->dx;
-  a.dy = h->dy;
-  a.rdx = h->rdx;
-  a.rdy = h->rdy;
-  a.dt = dt;
-  a.stage = st;
-  a.b = st == 2 ? 0.75 : (st == 3 ? 1.0 / 3.0 : 0.0);  // rk3tvd_steps_module.f:225,444
-  a.periodic = h->periodic;
-  a.k = h->k;
+  StageArgs a = make_stage_args(h, uin, uout, dt, st);
   prof_begin(h);
   cudaError_t e = launch_interior_stage(a, h->stream);
   prof_end(h);

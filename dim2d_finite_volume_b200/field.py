@@ -74,6 +74,10 @@ def _preset(name):
     elif name == "hedstrom_xy":
         ch = {s: HEDSTROM for s in SIDES}
         order = ["SW", "S", "SE", "W", "E", "NW", "N", "NE"]
+    elif name == "wall_S_reflection":  # library_config.py:102-115
+        ch = dict(N=REFLECTION_Y, S=WALL, E=REFLECTION_X, W=REFLECTION_X, NE=REFLECTION_X,
+                  NW=REFLECTION_X, SE=REFLECTION_X, SW=REFLECTION_X)
+        order = ["W", "E", "S", "N", "SW", "SE", "NW", "NE"]
     elif name == "reflection_xy":
         ch = dict(N=REFLECTION_Y, S=REFLECTION_Y, E=REFLECTION_X, W=REFLECTION_X,
                   NE=REFLECTION_Y, NW=REFLECTION_Y, SE=REFLECTION_Y, SW=REFLECTION_Y)

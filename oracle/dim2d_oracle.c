@@ -707,10 +707,11 @@ int orc_integrate(const orc_cfg *c, double *nodes, const double *x_map, const do
     orc_apply_bc_on_nodes(c, *t, x_map, y_map, nodes_tmp, nodes);
 
     *t = *t + dt;
+    if (orc_status()) break; /* the reference stops the program here */
   }
   free(nodes_tmp);
   free(time_dev);
-  return 0;
+  return orc_status();
 }
 
 /* field_abstract_class.f:286-315 */

@@ -109,6 +109,27 @@ void orc_ini_coordinates(int nx, int ny, double x_min, double x_max,
 /* debug_real = NF90_FILL_DOUBLE, parameters_input.f:892 */
 double orc_debug_real(void);
 
+/* wall operator status: 0 ok, 1 root not bracketed, 2-4 Ridders failures
+ * (where the reference stops the program) */
+int orc_status(void);
+void orc_clear_status(void);
+
+/* wall_xy_equilibrium_module.f unit functions (known-answer tests) */
+double orc_md_vapor(double T);
+double orc_md_liquid(double T);
+double orc_dwall_internal_energy_dmd(double md, double T, double micro_angle);
+double orc_temperature_average(double T0, double delta_x, double q);
+double orc_wall_temperature(double md, double g2, double vx, double vy, double Ed);
+double orc_dmddx(double delta, const double tab[3], int grad_type);
+double orc_wall_equilibrium_root_fct(double md, const double md_x[2], const double md_y[2],
+                                     double vx, double vy, double Ed, double delta_x,
+                                     double delta_y, double micro_angle, double q,
+                                     int grad_type_x, int grad_type_y);
+double orc_wall_heat_flux(double t, double x, double y);
+/* compute_wall_flux_x at face (i,j) with the interior operators */
+void orc_wall_flux_x_at(const double *nodes, int nx, int ny, int i, int j, double t,
+                        const double *x_map, const double *y_map, int side_right, double f[4]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -204,6 +204,65 @@ def periodic(ref):
     }
 
 
+def wall(ref):
+    """test_bc_operators/test_wall_xy_equilibrium.f: the known answers that
+    the test constant set reproduces (capillarity parts of the wall flux at
+    face (4,3) of get_nodes_for_flux_test :349-381, and the unit functions
+    dwallInternalEnergy_dmd, temperature, dmddx, md_average :978-1060)."""
+    path = os.path.join(ref, "src/test_files/test_bc_operators/test_wall_xy_equilibrium.f")
+    src = open(path).read()
+    body = src[src.index("subroutine get_nodes_for_flux_test"):]
+    body = body[:body.index("end subroutine get_nodes_for_flux_test")]
+    assign = []
+    for m in re.finditer(r"nodes\((\d+):(\d+),(\d+),(\d+)\)\s*=\s*\[([^\]]*)\]", body):
+        vals = [fnum(t) for t in re.findall(NUM, m.group(5))]
+        assign.append({"i": [int(m.group(1)), int(m.group(2))], "j": int(m.group(3)),
+                       "k": int(m.group(4)), "values": vals})
+    m = re.search(r"nodes\((\d+),(\d+),(\d+)\)\s*=\s*(%s)" % NUM, body)
+    assign.append({"i": [int(m.group(1)), int(m.group(1))], "j": int(m.group(2)),
+                   "k": int(m.group(3)), "values": [fnum(m.group(4))]})
+    fill = fnum(re.search(r"nodes\(i,j,k\)\s*=\s*(%s)" % NUM, body).group(1))
+
+    def expect(fn_name):
+        blk = src[src.index("function test_%s(" % fn_name):]
+        blk = blk[:blk.index("end function test_%s" % fn_name)]
+        lits = re.findall(r",\s*\$?\s*(%s)d0,\s*\$?\s*detailled" % NUM, blk.replace("\n", " "))
+        return fnum(lits[-1] + "d0")
+
+    def call_args(fn_name, callee):
+        blk = src[src.index("function test_%s(" % fn_name):]
+        blk = blk[:blk.index("end function test_%s" % fn_name)].replace("\n", " ")
+        blk = re.sub(r"\s*\$\s*", " ", blk)
+        start = re.search(r"[^\w]%s\(" % callee, blk[blk.index("result("):]).end()
+        inner = blk[blk.index("result("):][start:]
+        depth, out = 1, ""
+        for ch in inner:
+            depth += ch == "("
+            depth -= ch == ")"
+            if depth == 0:
+                break
+            out += ch
+        return out
+
+    dE_args = [fnum(t) for t in re.findall(NUM, call_args("dwallInternalEnergy_dmd",
+                                                          "dwallInternalEnergy_dmd"))]
+    T_args = [fnum(t) for t in re.findall(NUM, call_args("temperature", "temperature"))]
+    dm = call_args("dmddx", "dmddx")
+    dm_args = [fnum(t) for t in re.findall(NUM, dm)]
+    av_args = [fnum(t) for t in re.findall(NUM, call_args("md_average", "md_average"))]
+    return {
+        "source": "src/test_files/test_bc_operators/test_wall_xy_equilibrium.f",
+        "flux_nodes": {"shape": [5, 5, 4], "fill": fill, "assign": assign, "dx": 0.1, "dy": 0.2,
+                       "face": [4, 3]},
+        "flux_x_capillarity_momentum_x": expect("flux_x_capillarity_momentum_x"),
+        "flux_x_capillarity_momentum_y": expect("flux_x_capillarity_momentum_y"),
+        "dwallInternalEnergy_dmd": {"args": dE_args, "value": expect("dwallInternalEnergy_dmd")},
+        "temperature": {"args": T_args, "value": expect("temperature")},
+        "dmddx": {"args": dm_args, "grad_type": "sd_interior_type", "value": expect("dmddx")},
+        "md_average": {"args": av_args, "value": expect("md_average")},
+    }
+
+
 def main():
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     out = {
@@ -211,6 +270,7 @@ def main():
         "dim2d_fluxes.json": dim2d_fluxes(ref),
         "hedstrom_xy.json": hedstrom(ref),
         "periodic_xy.json": periodic(ref),
+        "wall_xy_equilibrium.json": wall(ref),
     }
     for name, obj in out.items():
         with open(os.path.join(HERE, name), "w") as fh:

@@ -115,3 +115,41 @@ def test_periodic_ghost_known_answers(oracle):
         want = _fortran_array(b)  # [k][j][i] for the block
         got = nodes[:3, b["j"][0] - 1:b["j"][1], b["i"][0] - 1:b["i"][1]]
         assert np.array_equal(got, want), b
+
+
+def test_wall_known_answers(oracle):
+    """wall_xy_equilibrium_module.f unit functions and the capillarity parts
+    of the wall x-flux (test_bc_operators/test_wall_xy_equilibrium.f)."""
+    import ctypes
+    w = json.load(open(os.path.join(GOLD, "wall_xy_equilibrium.json")))
+    oracle.set_params(re=5.0, we=10.0, pr=20.0, cv_r=2.5, viscous_r=-1.5)
+    L = oracle.lib()
+    d, dp = ctypes.c_double, ctypes.POINTER(ctypes.c_double)
+    L.orc_dwall_internal_energy_dmd.restype = d
+    L.orc_dwall_internal_energy_dmd.argtypes = [d, d, d]
+    L.orc_wall_temperature.restype = d
+    L.orc_wall_temperature.argtypes = [d] * 5
+    L.orc_dmddx.restype = d
+    L.orc_dmddx.argtypes = [d, dp, ctypes.c_int]
+    L.orc_wall_capillarity_x.restype = d
+    L.orc_wall_capillarity_x.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, d, d, ctypes.c_int]
+    e = w["dwallInternalEnergy_dmd"]
+    assert abs(L.orc_dwall_internal_energy_dmd(*e["args"]) - e["value"]) < 5e-10
+    e = w["temperature"]
+    assert abs(L.orc_wall_temperature(*e["args"]) - e["value"]) < 1e-12
+    e = w["dmddx"]
+    tab = np.array(e["args"][1:])
+    assert L.orc_dmddx(e["args"][0], oracle.ptr(tab), 0) == e["value"]
+    e = w["md_average"]
+    assert 0.5 * (e["args"][0] + e["args"][1]) == e["value"]
+    fn = w["flux_nodes"]
+    nodes = np.full((4, 5, 5), fn["fill"])
+    for a in fn["assign"]:
+        i0, i1 = a["i"]
+        nodes[a["k"] - 1, a["j"] - 1, i0 - 1:i1] = a["values"]
+    i, j = fn["face"]
+    got_x = L.orc_wall_capillarity_x(oracle.ptr(nodes), 5, 5, i, j, fn["dx"], fn["dy"], 0)
+    got_y = L.orc_wall_capillarity_x(oracle.ptr(nodes), 5, 5, i, j, fn["dx"], fn["dy"], 1)
+    assert abs(got_x - w["flux_x_capillarity_momentum_x"]) < 1e-9
+    assert abs(got_y - w["flux_x_capillarity_momentum_y"]) < 1e-10
