@@ -33,6 +33,9 @@ sys.path.insert(0, ROOT)
 N_INTERIOR = 1024
 BYTES_PER_CELL_UPDATE = 256  # 3 stage writes + 3 stage reads + 2 reads of u^n, 32 B each
 L2_BYTES = 126 * 1024 * 1024
+# stage-kernel variants of the library (dim2d_set_variant)
+STAGE_KERNELS = ["k_interior<1> 32x8 tiles", "k_strip<8,4,1>", "k_strip<16,4,1>",
+                 "k_strip<32,4,1>", "k_strip<16,8,1>", "k_strip<8,8,1>"]
 
 
 def parse():
@@ -44,6 +47,8 @@ def parse():
     ap.add_argument("--n", type=int, default=N_INTERIOR)
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--bc", default="hedstrom_xy", choices=["hedstrom_xy", "periodic_xy"])
+    ap.add_argument("--variant", default="auto",
+                    help="stage-kernel variant 0..5, or 'auto' (the library's autotuner)")
     ap.add_argument("--cpu-budget", type=float, default=15.0,
                     help="seconds of host time for the cpu_baseline sample")
     return ap.parse_args()
@@ -259,6 +264,12 @@ def main():
     fld = F.Field(nx, ny, bc=a.bc)
     fld.set_stream(stream.cuda_stream)
     fld.ini(w["nodes"], w["x_map"], w["y_map"])
+    tune_ms = None
+    if a.variant == "auto":
+        _, tune_ms = fld.autotune(measure=True)  # before the timed region
+    else:
+        fld.variant = int(a.variant)
+    variant = fld.variant
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
 
     def barrier():
@@ -336,10 +347,12 @@ def main():
                                    "Mach %.1f flow, RK3 step" % (a.n, 0.1 if a.bc == "hedstrom_xy"
                                                                  else 0.0), "bc": a.bc, "nx": nx, "ny": ny, "dt": dt,
                        "l2": "flushed between timed steps (2x L2 write, outside the events)",
-                       "replicas_per_gpu": 1},
+                       "replicas_per_gpu": 1, "stage_kernel": STAGE_KERNELS[variant],
+                       "autotune_ms": (None if tune_ms is None
+                                       else [round(float(x), 5) for x in tune_ms])},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
-                         "kernel": "k_interior<1> (fused RK3 stage)",
+                         "kernel": STAGE_KERNELS[variant] + " (fused RK3 stage)",
                          "algorithmic_bytes_per_launch": bytes_per_launch,
                          "launch_ms": per_launch_ms,
                          "traffic": (tr * cells if tr is not None else None)},

@@ -7,6 +7,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 
 #include "../../include/dim2d.h"
@@ -17,6 +19,9 @@ using namespace dim2d;
 
 namespace {
 thread_local std::string g_last_error;
+// autotuner cache: (nx, ny, boundary class) -> variant
+std::mutex g_tune_mu;
+std::map<long long, int> g_tune;
 }
 
 namespace dim2d {
@@ -326,6 +331,74 @@ int dim2d_device_state(dim2d_handle* h, double** nodes, int* pitch) {
 }
 
 long long dim2d_launch_count(const dim2d_handle* h) { return h ? h->launches : 0; }
+
+int dim2d_set_variant(dim2d_handle* h, int variant) {
+  if (!h) return set_error(DIM2D_ERR_ARG, "set_variant: null handle");
+  if (variant < 0 || variant >= NUM_VARIANTS)
+    return set_error(DIM2D_ERR_ARG, "set_variant: variant %d out of range", variant);
+  h->variant = variant;
+  return DIM2D_OK;
+}
+
+int dim2d_get_variant(const dim2d_handle* h) { return h ? h->variant : -1; }
+
+int dim2d_autotune(dim2d_handle* h, int* chosen, double* times_ms) {
+  if (!h) return set_error(DIM2D_ERR_ARG, "autotune: null handle");
+  if (!h->uploaded) return set_error(DIM2D_ERR_NOT_READY, "autotune: no state");
+  const int cls = h->periodic ? 0 : (h->open_all ? 1 : (h->south_wall ? 2 : 3));
+  const long long key = ((long long)h->f.nx << 32) ^ ((long long)h->f.ny << 4) ^ cls;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end() && !times_ms) {
+      h->variant = it->second;
+      if (chosen) *chosen = h->variant;
+      return DIM2D_OK;
+    }
+  }
+  cudaError_t e = cudaSuccess;
+  if (!h->td) e = cudaMalloc(&h->td, 4 * h->f.plane * sizeof(double));
+  if (e != cudaSuccess) return set_error(DIM2D_ERR_NOMEM, "autotune: %s", cudaGetErrorString(e));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int best = 0;
+  double best_ms = 1e30;
+  const int saved = h->variant;
+  for (int v = 0; v < NUM_VARIANTS; v++) {
+    h->variant = v;
+    const StageArgs a = make_stage_args(h, h->A, h->td, 0.0, 0);
+    for (int w = 0; w < 2 && e == cudaSuccess; w++) e = launch_time_dev(a, h->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, h->stream);
+    const int reps = 5;
+    for (int r = 0; r < reps && e == cudaSuccess; r++) e = launch_time_dev(a, h->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, h->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    h->launches += 2 + reps;
+    if (e != cudaSuccess) break;
+    const double per = ms / reps;
+    if (times_ms) times_ms[v] = per;
+    if (per < best_ms) {
+      best_ms = per;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) {
+    h->variant = saved;
+    return cuda_error(e, "autotune");
+  }
+  h->variant = best;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune[key] = best;
+  }
+  if (chosen) *chosen = best;
+  return DIM2D_OK;
+}
 
 int dim2d_profile(dim2d_handle* h, int enable) {
   if (!h) return set_error(DIM2D_ERR_ARG, "profile: null handle");

@@ -45,6 +45,7 @@ struct StageArgs {
   int stage;                       // 1, 2, 3
   int periodic;                    // write periodic ghost images of edge cells
   int wall_w, wall_e, wall_s, wall_n;  // wall flux override on that side
+  int variant;                         // 0 = 32x8 CTA tiles, 1..5 = warp strips (shape-1)
   double t;                            // field time (constant over the stages)
   double xmap0, ymap0;                 // x_map(1), y_map(1): x_map(i) = xmap0 + (i-1) dx
   WallConst wall;
@@ -73,6 +74,10 @@ constexpr int TILE_Y = 8;
 size_t interior_smem_bytes();
 
 cudaError_t launch_interior_stage(const StageArgs& a, cudaStream_t s);
+// warp-streaming variant (dim2d_strip.cu); mode 0 = L(u), 1 = stage update;
+// shape 0..4 = strip height / warps per CTA (8,4) (16,4) (32,4) (16,8) (8,8)
+cudaError_t launch_strip_stage(const StageArgs& a, int mode, int shape, cudaStream_t s);
+constexpr int NUM_VARIANTS = 6;
 // L(a.uin) of the interior cells into a.uout (stage fields ignored)
 cudaError_t launch_time_dev(const StageArgs& a, cudaStream_t s);
 // open (Hedstrom) ghost cells of a field open on all sides; mode 0 writes

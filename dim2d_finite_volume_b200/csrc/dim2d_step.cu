@@ -30,6 +30,7 @@ StageArgs make_stage_args(const dim2d_handle* h, const double* uin, double* uout
   a.b = st == 2 ? 0.75 : (st == 3 ? 1.0 / 3.0 : 0.0);  // rk3tvd_steps_module.f:225,444
   a.periodic = h->periodic;
   a.wall_s = h->south_wall;
+  a.variant = h->variant;
   a.t = h->t;
   a.xmap0 = h->xmap0;
   a.ymap0 = h->ymap0;

@@ -134,6 +134,9 @@ def library():
         "dim2d_profile": (ctypes.c_int, [H, ctypes.c_int]),
         "dim2d_profile_read": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_double),
                                               ctypes.POINTER(ctypes.c_longlong)]),
+        "dim2d_set_variant": (ctypes.c_int, [H, ctypes.c_int]),
+        "dim2d_get_variant": (ctypes.c_int, [H]),
+        "dim2d_autotune": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_int), _dp]),
         "dim2d_destroy": (ctypes.c_int, [H]),
         "dim2d_ini_coordinates": (ctypes.c_int, [ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 4
                                   + [_dp, _dp]),
@@ -264,6 +267,26 @@ class Field:
     @property
     def launches(self):
         return library().dim2d_launch_count(self._h)
+
+    NUM_VARIANTS = 6
+
+    @property
+    def variant(self):
+        """Stage-kernel variant in use (0 = CTA tiles, 1..5 = warp strips)."""
+        return library().dim2d_get_variant(self._h)
+
+    @variant.setter
+    def variant(self, v):
+        _check(library().dim2d_set_variant(self._h, int(v)))
+
+    def autotune(self, measure=False):
+        """Time every stage-kernel variant on the resident field and keep
+        the fastest; returns (variant, per-variant ms or None)."""
+        chosen = ctypes.c_int()
+        times = np.zeros(self.NUM_VARIANTS) if measure else None
+        ptr = times.ctypes.data_as(_dp) if measure else None
+        _check(library().dim2d_autotune(self._h, ctypes.byref(chosen), ptr))
+        return chosen.value, times
 
     def close(self):
         if getattr(self, "_h", None):

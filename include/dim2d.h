@@ -167,6 +167,21 @@ DIM2D_API long long dim2d_launch_count(const dim2d_handle *h);
 DIM2D_API int dim2d_profile(dim2d_handle *h, int enable);
 DIM2D_API int dim2d_profile_read(dim2d_handle *h, double *ms, long long *launches);
 
+/* No counterpart in the reference (its stage loops have one fixed shape).
+ * Stage-kernel variant: 0 = 32x8-cell CTA tiles; 1..5 = warp-streaming
+ * strips 31 columns wide with (rows per warp, warps per CTA) = (8,4),
+ * (16,4), (32,4), (16,8), (8,8).  Every variant evaluates the same face
+ * fluxes with the same formulas; results agree to rounding. */
+#define DIM2D_NUM_VARIANTS 6
+DIM2D_API int dim2d_set_variant(dim2d_handle *h, int variant);
+DIM2D_API int dim2d_get_variant(const dim2d_handle *h);
+/* Autotuner: times every variant on the resident field (time-derivative
+ * launches; the state is not modified), selects the fastest and caches the
+ * choice for fields of the same size and boundary class in this process.
+ * times_ms (optional, DIM2D_NUM_VARIANTS entries) receives the average
+ * launch time of each variant; passing it forces a new measurement. */
+DIM2D_API int dim2d_autotune(dim2d_handle *h, int *chosen, double *times_ms);
+
 DIM2D_API int dim2d_destroy(dim2d_handle *h);
 
 /* No counterpart in the reference.  The RK3 time step for callers that
