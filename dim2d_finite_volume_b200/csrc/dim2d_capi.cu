@@ -367,16 +367,16 @@ int dim2d_autotune(dim2d_handle* h, int* chosen, double* times_ms) {
   const int saved = h->variant;
   for (int v = 0; v < NUM_VARIANTS; v++) {
     h->variant = v;
+    // the whole stage work: stage kernel (+ ghost kernel where not fused)
     const StageArgs a = make_stage_args(h, h->A, h->td, 0.0, 0);
-    for (int w = 0; w < 2 && e == cudaSuccess; w++) e = launch_time_dev(a, h->stream);
+    for (int w = 0; w < 2 && e == cudaSuccess; w++) e = launch_stage_work(h, a, 0);
     if (e == cudaSuccess) e = cudaEventRecord(e0, h->stream);
     const int reps = 5;
-    for (int r = 0; r < reps && e == cudaSuccess; r++) e = launch_time_dev(a, h->stream);
+    for (int r = 0; r < reps && e == cudaSuccess; r++) e = launch_stage_work(h, a, 0);
     if (e == cudaSuccess) e = cudaEventRecord(e1, h->stream);
     if (e == cudaSuccess) e = cudaEventSynchronize(e1);
     float ms = 0.f;
     if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
-    h->launches += 2 + reps;
     if (e != cudaSuccess) break;
     const double per = ms / reps;
     if (times_ms) times_ms[v] = per;
@@ -439,16 +439,9 @@ int dim2d_time_dev(dim2d_handle* h, double* time_dev) {
   // td_operators_class.f:150-154: every cell starts at debug_real
   e = launch_fill(h->td, 9.9692099683868690e+36, 4 * f.plane, h->stream);
   h->launches++;
-  const StageArgs a = make_stage_args(h, h->A, h->td, 0.0, 0);
-  if (e == cudaSuccess) {
-    e = launch_time_dev(a, h->stream);
-    h->launches++;
-  }
-  if (e == cudaSuccess && h->open_all) {
-    // bc_operators_hedstrom_xy_class.f:182-496: ghost-cell time derivatives
-    e = launch_open_ghosts(a, 0, h->stream);
-    h->launches++;
-  }
+  // interior cells, and on open fields the ghost cells
+  // (bc_operators_hedstrom_xy_class.f:182-496)
+  if (e == cudaSuccess) e = launch_stage_work(h, make_stage_args(h, h->A, h->td, 0.0, 0), 0);
   if (e != cudaSuccess) return cuda_error(e, "time_dev");
   e = cudaMemcpy2DAsync(time_dev, f.nx * sizeof(double), h->td, f.pitch * sizeof(double),
                         f.nx * sizeof(double), 4 * (size_t)f.ny, cudaMemcpyDeviceToHost,

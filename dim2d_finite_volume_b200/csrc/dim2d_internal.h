@@ -72,6 +72,10 @@ WallConst make_wall(const dim2d_params& p);
 dim2d::StageArgs make_stage_args(const dim2d_handle* h, const double* uin, double* uout,
                                  double dt, int st);
 int rk3_step(dim2d_handle* h, double dt);
+// the complete work of one stage (mode 1) or time derivative (mode 0): the
+// stage kernel and, on open fields where the stage kernel does not cover
+// them, the ghost-cell kernel; counts launches, profiles the stage kernel
+cudaError_t launch_stage_work(dim2d_handle* h, const dim2d::StageArgs& a, int mode);
 int apply_bc_on_nodes(dim2d_handle* h, const double* nodes_tmp, double* nodes);
 int check_status(dim2d_handle* h);
 // bracket one launch with profiling events (no-op unless h->prof)

@@ -46,6 +46,8 @@ struct StageArgs {
   int periodic;                    // write periodic ghost images of edge cells
   int wall_w, wall_e, wall_s, wall_n;  // wall flux override on that side
   int variant;                         // 0 = 32x8 CTA tiles, 1..5 = warp strips (shape-1)
+  int open;                            // all sides open: strip launches also integrate the
+                                       // ghost cells (their first CTAs)
   double t;                            // field time (constant over the stages)
   double xmap0, ymap0;                 // x_map(1), y_map(1): x_map(i) = xmap0 + (i-1) dx
   WallConst wall;
@@ -77,6 +79,8 @@ cudaError_t launch_interior_stage(const StageArgs& a, cudaStream_t s);
 // warp-streaming variant (dim2d_strip.cu); mode 0 = L(u), 1 = stage update;
 // shape 0..4 = strip height / warps per CTA (8,4) (16,4) (32,4) (16,8) (8,8)
 cudaError_t launch_strip_stage(const StageArgs& a, int mode, int shape, cudaStream_t s);
+// 1 if the stage launch of `a` also covers the open-boundary ghost cells
+inline bool stage_fuses_open(const StageArgs& a) { return a.open && a.variant > 0; }
 constexpr int NUM_VARIANTS = 6;
 // L(a.uin) of the interior cells into a.uout (stage fields ignored)
 cudaError_t launch_time_dev(const StageArgs& a, cudaStream_t s);

@@ -31,6 +31,7 @@ StageArgs make_stage_args(const dim2d_handle* h, const double* uin, double* uout
   a.periodic = h->periodic;
   a.wall_s = h->south_wall;
   a.variant = h->variant;
+  a.open = h->open_all;
   a.t = h->t;
   a.xmap0 = h->xmap0;
   a.ymap0 = h->ymap0;
@@ -110,23 +111,25 @@ int check_status(dim2d_handle* h) {
   return DIM2D_OK;
 }
 
-static int stage(dim2d_handle* h, int st, const double* uin, double* uout, double dt) {
-  StageArgs a = make_stage_args(h, uin, uout, dt, st);
+cudaError_t launch_stage_work(dim2d_handle* h, const StageArgs& a, int mode) {
   prof_begin(h);
-  cudaError_t e = launch_interior_stage(a, h->stream);
+  cudaError_t e = mode == 0 ? launch_time_dev(a, h->stream) : launch_interior_stage(a, h->stream);
   prof_end(h);
   h->launches++;
-  if (e != cudaSuccess) return cuda_error(e, "rk3 stage");
-  if (h->periodic) return DIM2D_OK;  // ghost images written by the stage kernel
-  if (h->open_all) {
-    // every ghost cell has a time derivative and is integrated like the
-    // interior (x/y_borders widened, field_abstract_class.f:244-270); no
-    // node boundary pass follows
-    e = launch_open_ghosts(a, 1, h->stream);
+  if (e == cudaSuccess && a.open && !stage_fuses_open(a)) {
+    e = launch_open_ghosts(a, mode, h->stream);
     h->launches++;
-    if (e != cudaSuccess) return cuda_error(e, "rk3 stage (open ghosts)");
-    return DIM2D_OK;
   }
+  return e;
+}
+
+static int stage(dim2d_handle* h, int st, const double* uin, double* uout, double dt) {
+  // on open fields every ghost cell has a time derivative and is integrated
+  // like the interior (x/y_borders widened, field_abstract_class.f:244-270)
+  // and no node boundary pass follows
+  cudaError_t e = launch_stage_work(h, make_stage_args(h, uin, uout, dt, st), 1);
+  if (e != cudaSuccess) return cuda_error(e, "rk3 stage");
+  if (h->periodic || h->open_all) return DIM2D_OK;  // periodic images: by the stage kernel
   return apply_bc_on_nodes(h, h->A, uout);
 }
 

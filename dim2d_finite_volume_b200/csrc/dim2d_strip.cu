@@ -17,7 +17,12 @@
 // Lane 31 computes only the x-face its left neighbour needs.  Warps are
 // independent (__syncwarp only), so the latency of one warp's loads is
 // hidden by the arithmetic of the others.
-#include "dim2d_kernels.cuh"
+//
+// On a field open on all sides the launch also integrates the ghost cells
+// (open_ghost_cell, one thread each): they take the first CTAs of the
+// grid, so their long dependent chains start first and overlap the strips.
+// Ghost and interior cells read the same input and write disjoint cells.
+#include "dim2d_open.cuh"
 
 namespace dim2d {
 
@@ -187,14 +192,27 @@ __device__ __forceinline__ void y_face(const StageArgs& a, const Ring& R, int la
   G[3] = F[3];
 }
 
-template <int H, int WPC, int MODE, bool WALL>
-__global__ void __launch_bounds__(32 * WPC) k_strip(StageArgs a) {
+// boundary kinds of the strip kernel
+enum StripKind : int { K_PLAIN = 0, K_WALL = 1, K_OPEN = 2 };
+
+// grid: [ghost CTAs (K_OPEN only)] + sx * sy strip CTAs, x fastest
+template <int H, int WPC, int MODE, int KIND>
+__global__ void __launch_bounds__(32 * WPC) k_strip(StageArgs a, int ghost_ctas, int sx) {
+  constexpr bool WALL = KIND == K_WALL;
+  int b = blockIdx.x;
+  if (KIND == K_OPEN) {
+    if (b < ghost_ctas) {
+      open_ghost_cell(a, b * (32 * WPC) + threadIdx.x, MODE);
+      return;
+    }
+    b -= ghost_ctas;
+  }
   extern __shared__ __align__(16) double sm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const Ring R{sm + warp * WARP_DOUBLES, sm + warp * WARP_DOUBLES + RR * 4 * RC};
   const Field f = a.f;
-  const int c0 = BC + blockIdx.x * SW;
-  const int y0 = BC + (blockIdx.y * WPC + warp) * H;
+  const int c0 = BC + (b % sx) * SW;
+  const int y0 = BC + ((b / sx) * WPC + warp) * H;
   const int ylast = f.ny - BC - 1;
   if (y0 > ylast) return;  // the whole warp leaves; no CTA barrier is used
   const int y1 = min(y0 + H, ylast + 1);
@@ -278,19 +296,28 @@ __global__ void __launch_bounds__(32 * WPC) k_strip(StageArgs a) {
   }
 }
 
+template <int H, int WPC, int MODE>
+const void* strip_fn(int kind) {
+  if (kind == K_WALL) return (const void*)k_strip<H, WPC, MODE, K_WALL>;
+  if (kind == K_OPEN) return (const void*)k_strip<H, WPC, MODE, K_OPEN>;
+  return (const void*)k_strip<H, WPC, MODE, K_PLAIN>;
+}
+
 template <int H, int WPC>
 cudaError_t launch_strip_shape(const StageArgs& a, int mode, cudaStream_t s) {
   const size_t smem = (size_t)WPC * WARP_DOUBLES * sizeof(double);
   const bool wall = a.wall_w || a.wall_e || a.wall_s || a.wall_n;
-  const void* fn;
-  if (mode == 0) fn = wall ? (const void*)k_strip<H, WPC, 0, true> : (const void*)k_strip<H, WPC, 0, false>;
-  else fn = wall ? (const void*)k_strip<H, WPC, 1, true> : (const void*)k_strip<H, WPC, 1, false>;
+  const int kind = a.open ? K_OPEN : (wall ? K_WALL : K_PLAIN);
+  const void* fn = mode == 0 ? strip_fn<H, WPC, 0>(kind) : strip_fn<H, WPC, 1>(kind);
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((a.f.nx - 2 * BC + SW - 1) / SW, (a.f.ny - 2 * BC + H * WPC - 1) / (H * WPC));
+  int sx = (a.f.nx - 2 * BC + SW - 1) / SW;
+  const int sy = (a.f.ny - 2 * BC + H * WPC - 1) / (H * WPC);
+  int ghost_ctas = kind == K_OPEN ? (open_ghost_count(a.f) + 32 * WPC - 1) / (32 * WPC) : 0;
+  const unsigned blocks = (unsigned)ghost_ctas + (unsigned)sx * (unsigned)sy;
   StageArgs aa = a;
-  void* args[] = {&aa};
-  return cudaLaunchKernel(fn, grid, dim3(32 * WPC), args, smem, s);
+  void* args[] = {&aa, &ghost_ctas, &sx};
+  return cudaLaunchKernel(fn, dim3(blocks), dim3(32 * WPC), args, smem, s);
 }
 
 }  // namespace
