@@ -34,8 +34,8 @@ N_INTERIOR = 1024
 BYTES_PER_CELL_UPDATE = 256  # 3 stage writes + 3 stage reads + 2 reads of u^n, 32 B each
 L2_BYTES = 126 * 1024 * 1024
 # stage-kernel variants of the library (dim2d_set_variant)
-STAGE_KERNELS = ["k_interior<1> 32x8 tiles", "k_strip<8,4,1>", "k_strip<16,4,1>",
-                 "k_strip<32,4,1>", "k_strip<16,8,1>", "k_strip<8,8,1>"]
+STAGE_KERNELS = ["k_interior<1> 32x8 tiles", "k_strip<8,4,4>", "k_strip<16,4,4>",
+                 "k_strip<16,4,5>", "k_strip<8,4,5>", "k_strip<16,8,2>"]
 
 
 def parse():

@@ -169,9 +169,9 @@ DIM2D_API int dim2d_profile_read(dim2d_handle *h, double *ms, long long *launche
 
 /* No counterpart in the reference (its stage loops have one fixed shape).
  * Stage-kernel variant: 0 = 32x8-cell CTA tiles; 1..5 = warp-streaming
- * strips 31 columns wide with (rows per warp, warps per CTA) = (8,4),
- * (16,4), (32,4), (16,8), (8,8).  Every variant evaluates the same face
- * fluxes with the same formulas; results agree to rounding. */
+ * strips 30 columns wide with (rows per warp, warps per CTA, resident CTAs
+ * per SM) = (8,4,4), (16,4,4), (16,4,5), (8,4,5), (16,8,2).  Every variant
+ * evaluates the same face fluxes; results agree to rounding. */
 #define DIM2D_NUM_VARIANTS 6
 DIM2D_API int dim2d_set_variant(dim2d_handle *h, int variant);
 DIM2D_API int dim2d_get_variant(const dim2d_handle *h);
