@@ -38,28 +38,27 @@ namespace {
 
 constexpr int SW = 30;  // cells per strip
 constexpr int RC = 34;  // state columns in the ring: c0-2 .. c0+31
-constexpr int PC = 32;  // node-quantity columns: c0-1 .. c0+30
+constexpr int PC = 34;  // node-quantity columns: c0-1 .. c0+32 (the last two are
+                        // padding read only by lane 31, whose faces are unused)
 constexpr int NS = 3;   // state rows (y .. y+2)
 constexpr int NUV = 3;  // velocity rows (y-1 .. y+1)
 constexpr int NQ = 2;   // rows of the other node quantities (y, y+1)
-enum NodeQ : int { Q_P = 0, Q_TCL, Q_CP, Q_TCAP, Q_LAP, Q_GX, Q_GY, NQV };
-constexpr int WARP_DOUBLES = NS * 4 * RC + NUV * 2 * PC + NQ * NQV * PC;
+// node quantities besides u, v; GXH/GYH = half the centred density
+// gradient, LAPH = half the density Laplacian
+enum NodeQ : int { Q_P = 0, Q_TCL, Q_CP, Q_TCAP, Q_LAPH, Q_GXH, Q_GYH, NQV };
+constexpr int ST_ROW = 4 * RC;    // doubles per state row (4 variables)
+constexpr int UV_ROW = 2 * PC;    // doubles per velocity row
+constexpr int Q_ROW = NQV * PC;   // doubles per node-quantity row
+constexpr int WARP_DOUBLES = NS * ST_ROW + NUV * UV_ROW + NQ * Q_ROW;
 
-// ring slots are selected by row number modulo the ring depth
-struct Ring {
-  double* st;  // [NS][4][RC]  rho, m_x, m_y, E
-  double* uv;  // [NUV][2][PC] u, v
-  double* q;   // [NQ][NQV][PC]
-  __device__ __forceinline__ double& r(int row, int v, int col) const {
-    return st[((row % NS) * 4 + v) * RC + col];
-  }
-  __device__ __forceinline__ double& u(int row, int c, int col) const {
-    return uv[((row % NUV) * 2 + c) * PC + col];
-  }
-  __device__ __forceinline__ double& n(int row, int c, int col) const {
-    return q[((row % NQ) * NQV + c) * PC + col];
-  }
-};
+extern __shared__ __align__(16) double g_ring[];
+
+// Ring rows are addressed by offsets into g_ring that already include the
+// warp's base and the lane's column; the offsets rotate as the warp moves
+// up, so every access below is a register plus a compile-time constant.
+#define ST(o, v, dc) g_ring[(o) + (v) * RC + (dc)]
+#define UV(o, c, dc) g_ring[(o) + (c) * PC + (dc)]
+#define NQ_(o, c, dc) g_ring[(o) + (c) * PC + (dc)]
 
 // global loads of the state row `row` for columns c0-2+lane and c0+30+lane
 __device__ __forceinline__ void load_row(const StageArgs& a, int c0, int row, int lane,
@@ -80,80 +79,77 @@ __device__ __forceinline__ void load_row(const StageArgs& a, int c0, int row, in
   }
 }
 
-__device__ __forceinline__ void store_row(const Ring& R, int row, int lane, const double v[2][4]) {
+// state row into the ring row at offset o (lane's column 0 = c0-2+lane)
+__device__ __forceinline__ void store_row(int o, int lane, const double v[2][4]) {
 #pragma unroll
-  for (int s = 0; s < 2; s++) {
-    const int col = lane + 32 * s;
-    if (col < RC) {
+  for (int q = 0; q < 4; q++) ST(o, q, 0) = v[0][q];
+  if (lane + 32 < RC) {
 #pragma unroll
-      for (int q = 0; q < 4; q++) R.r(row, q, col) = v[s][q];
-    }
+    for (int q = 0; q < 4; q++) ST(o, q, 32) = v[1][q];
   }
 }
 
-// node quantities of row `row`, column c0-1+lane (needs state rows
-// row-1..row+1).  Primitives as node_prim() (dim2d_prim_module.f:242-289,
-// 425-453, 515-544, 1056-1071) with 1/rho and 1/(3-rho) from one division;
-// Tcap = 0.5/rho |grad rho|^2 with centred gradients (:582-613).
-__device__ __forceinline__ void node_row(const Ring& R, int row, int lane, double hrdx,
-                                         double hrdy, double rdx2, double rdy2,
+// node quantities of column c0-1+lane of one row: sm/s0/sp = state rows
+// below / at / above, ou/oq = output rows.  Primitives as node_prim()
+// (dim2d_prim_module.f:242-289, 425-453, 515-544, 1056-1071) with 1/rho
+// and 1/(3-rho) from one division; Tcap = 0.5/rho |grad rho|^2 with
+// centred gradients (:582-613).
+__device__ __forceinline__ void node_row(int sm, int s0, int sp, int ou, int oq, double qrdx,
+                                         double qrdy, double hrdx2, double hrdy2,
                                          const DimConst& k) {
-  const int pc = lane, rc = lane + 1;
-  const double r = R.r(row, 0, rc);
-  const double rw = R.r(row, 0, rc - 1), re = R.r(row, 0, rc + 1);
-  const double rs = R.r(row - 1, 0, rc), rn = R.r(row + 1, 0, rc);
+  const double r = ST(s0, 0, 1);
+  const double rw = ST(s0, 0, 0), re = ST(s0, 0, 2);
+  const double rs = ST(sm, 0, 1), rn = ST(sp, 0, 1);
   const double tm = 3.0 - r;
   const double inv = 1.0 / (r * tm);
   const double ir = tm * inv;
   const double cp = r * inv;
-  const double u = R.r(row, 1, rc) * ir, v = R.r(row, 2, rc) * ir;
-  const double w = R.r(row, 3, rc) - 0.5 * r * (u * u + v * v) + 3.0 * (r * r);
-  const double gx = hrdx * (re - rw), gy = hrdy * (rn - rs);
-  R.u(row, 0, pc) = u;
-  R.u(row, 1, pc) = v;
-  R.n(row, Q_P, pc) = k.c3cv * cp * w - 3.0 * (r * r);
-  R.n(row, Q_TCL, pc) = ir * w;
-  R.n(row, Q_CP, pc) = cp;
-  R.n(row, Q_TCAP, pc) = 0.5 * ir * (gx * gx + gy * gy);
-  R.n(row, Q_LAP, pc) = rdx2 * ((rw - 2.0 * r) + re) + rdy2 * ((rs - 2.0 * r) + rn);
-  R.n(row, Q_GX, pc) = gx;
-  R.n(row, Q_GY, pc) = gy;
+  const double u = ST(s0, 1, 1) * ir, v = ST(s0, 2, 1) * ir;
+  const double w = ST(s0, 3, 1) - 0.5 * r * (u * u + v * v) + 3.0 * (r * r);
+  const double gxh = qrdx * (re - rw), gyh = qrdy * (rn - rs);
+  UV(ou, 0, 0) = u;
+  UV(ou, 1, 0) = v;
+  NQ_(oq, Q_P, 0) = k.c3cv * cp * w - 3.0 * (r * r);
+  NQ_(oq, Q_TCL, 0) = ir * w;
+  NQ_(oq, Q_CP, 0) = cp;
+  NQ_(oq, Q_TCAP, 0) = 2.0 * ir * (gxh * gxh + gyh * gyh);
+  NQ_(oq, Q_LAPH, 0) = hrdx2 * ((rw - 2.0 * r) + re) + hrdy2 * ((rs - 2.0 * r) + rn);
+  NQ_(oq, Q_GXH, 0) = gxh;
+  NQ_(oq, Q_GYH, 0) = gyh;
 }
 
-// x-face between columns x-1 and x of row y, evaluated for column
-// c0 + l (l = the lane, clamped to SW)
+// x-face between columns x-1 and x of row y: s0 = state row y, um/u0/up =
+// velocity rows y-1, y, y+1, q0 = node row y
 template <bool WALL>
-__device__ __forceinline__ void x_face(const StageArgs& a, const Ring& R, int l, int x, int y,
-                                       double F[4]) {
+__device__ __forceinline__ void x_face(const StageArgs& a, int s0, int um, int u0, int up, int q0,
+                                       int x, double F[4]) {
   const DimConst& k = a.k;
-  const int rL = l + 1, rR = l + 2;  // state columns of L, R
-  const int pL = l, pR = l + 1;      // node-quantity columns
   FaceIn fi;
-  fi.ra = R.r(y, 0, rL); fi.rb = R.r(y, 0, rR);
-  fi.mna = R.r(y, 1, rL); fi.mnb = R.r(y, 1, rR);
-  fi.mta = R.r(y, 2, rL); fi.mtb = R.r(y, 2, rR);
-  fi.ea = R.r(y, 3, rL); fi.eb = R.r(y, 3, rR);
-  fi.una = R.u(y, 0, pL); fi.unb = R.u(y, 0, pR);
-  fi.uta = R.u(y, 1, pL); fi.utb = R.u(y, 1, pR);
-  fi.pa = R.n(y, Q_P, pL); fi.pb = R.n(y, Q_P, pR);
-  fi.ta = R.n(y, Q_TCL, pL); fi.tb = R.n(y, Q_TCL, pR);
-  fi.ca = R.n(y, Q_CP, pL); fi.cb = R.n(y, Q_CP, pR);
-  fi.ka = R.n(y, Q_TCAP, pL); fi.kb = R.n(y, Q_TCAP, pR);
+  fi.ra = ST(s0, 0, 1); fi.rb = ST(s0, 0, 2);
+  fi.mna = ST(s0, 1, 1); fi.mnb = ST(s0, 1, 2);
+  fi.mta = ST(s0, 2, 1); fi.mtb = ST(s0, 2, 2);
+  fi.ea = ST(s0, 3, 1); fi.eb = ST(s0, 3, 2);
+  fi.una = UV(u0, 0, 0); fi.unb = UV(u0, 0, 1);
+  fi.uta = UV(u0, 1, 0); fi.utb = UV(u0, 1, 1);
+  fi.pa = NQ_(q0, Q_P, 0); fi.pb = NQ_(q0, Q_P, 1);
+  fi.ta = NQ_(q0, Q_TCL, 0); fi.tb = NQ_(q0, Q_TCL, 1);
+  fi.ca = NQ_(q0, Q_CP, 0); fi.cb = NQ_(q0, Q_CP, 1);
+  fi.ka = NQ_(q0, Q_TCAP, 0); fi.kb = NQ_(q0, Q_TCAP, 1);
   const double rdx = a.rdx, q_rdy = 0.25 * a.rdy;
   fi.drn = rdx * (fi.rb - fi.ra);
-  fi.drt = 0.5 * (R.n(y, Q_GY, pL) + R.n(y, Q_GY, pR));
+  fi.drt = NQ_(q0, Q_GYH, 0) + NQ_(q0, Q_GYH, 1);
   fi.dunn = rdx * (fi.unb - fi.una);
-  fi.dunt = q_rdy * ((R.u(y + 1, 0, pL) + R.u(y + 1, 0, pR)) - (R.u(y - 1, 0, pL) + R.u(y - 1, 0, pR)));
+  fi.dunt = q_rdy * ((UV(up, 0, 0) + UV(up, 0, 1)) - (UV(um, 0, 0) + UV(um, 0, 1)));
   fi.dutn = rdx * (fi.utb - fi.uta);
-  fi.dutt = q_rdy * ((R.u(y + 1, 1, pL) + R.u(y + 1, 1, pR)) - (R.u(y - 1, 1, pL) + R.u(y - 1, 1, pR)));
-  fi.lap = 0.5 * (R.n(y, Q_LAP, pL) + R.n(y, Q_LAP, pR));
+  fi.dutt = q_rdy * ((UV(up, 1, 0) + UV(up, 1, 1)) - (UV(um, 1, 0) + UV(um, 1, 1)));
+  fi.lap = NQ_(q0, Q_LAPH, 0) + NQ_(q0, Q_LAPH, 1);
   fi.dtn = rdx * (fi.tb - fi.ta);
   fi.dkn = rdx * (fi.kb - fi.ka);
   const bool w_face = WALL && a.wall_w && x == BC;
   const bool e_face = WALL && a.wall_e && x == a.f.nx - BC;
   if (w_face || e_face) {
-    const int p = w_face ? pR : pL;
-    const double tl = k.c38cv * (R.n(y, Q_TCL, p) - k.iwe * R.n(y, Q_TCAP, p));
+    const int dc = w_face ? 1 : 0;
+    const double tl = k.c38cv * (NQ_(q0, Q_TCL, dc) - k.iwe * NQ_(q0, Q_TCAP, dc));
     const double q = wall_heat_flux(a.wall, a.xmap0 + x * a.dx);
     wall_face_flux(fi, tl, a.dx, q, w_face ? q : -q, k, F);
   } else {
@@ -161,41 +157,41 @@ __device__ __forceinline__ void x_face(const StageArgs& a, const Ring& R, int l,
   }
 }
 
-// y-face between rows yb and yb+1 of column c0 + l (l = the lane, clamped
-// to SW-1); output in conservative order (mass, m_x, m_y, E)
+// y-face between rows yb and yb+1 of column x: sb/st = state rows yb, yb+1,
+// ub/ut = velocity rows, qb/qt = node rows; output in conservative order
+// (mass, m_x, m_y, E)
 template <bool WALL>
-__device__ __forceinline__ void y_face(const StageArgs& a, const Ring& R, int l, int x, int yb,
-                                       double G[4]) {
+__device__ __forceinline__ void y_face(const StageArgs& a, int sb, int st, int ub, int ut, int qb,
+                                       int qt, int x, int yb, double G[4]) {
   const DimConst& k = a.k;
-  const int rc = l + 2, pc = l + 1;
   const int yt = yb + 1;
   FaceIn fi;
-  fi.ra = R.r(yb, 0, rc); fi.rb = R.r(yt, 0, rc);
-  fi.mna = R.r(yb, 2, rc); fi.mnb = R.r(yt, 2, rc);
-  fi.mta = R.r(yb, 1, rc); fi.mtb = R.r(yt, 1, rc);
-  fi.ea = R.r(yb, 3, rc); fi.eb = R.r(yt, 3, rc);
-  fi.una = R.u(yb, 1, pc); fi.unb = R.u(yt, 1, pc);
-  fi.uta = R.u(yb, 0, pc); fi.utb = R.u(yt, 0, pc);
-  fi.pa = R.n(yb, Q_P, pc); fi.pb = R.n(yt, Q_P, pc);
-  fi.ta = R.n(yb, Q_TCL, pc); fi.tb = R.n(yt, Q_TCL, pc);
-  fi.ca = R.n(yb, Q_CP, pc); fi.cb = R.n(yt, Q_CP, pc);
-  fi.ka = R.n(yb, Q_TCAP, pc); fi.kb = R.n(yt, Q_TCAP, pc);
+  fi.ra = ST(sb, 0, 2); fi.rb = ST(st, 0, 2);
+  fi.mna = ST(sb, 2, 2); fi.mnb = ST(st, 2, 2);
+  fi.mta = ST(sb, 1, 2); fi.mtb = ST(st, 1, 2);
+  fi.ea = ST(sb, 3, 2); fi.eb = ST(st, 3, 2);
+  fi.una = UV(ub, 1, 1); fi.unb = UV(ut, 1, 1);
+  fi.uta = UV(ub, 0, 1); fi.utb = UV(ut, 0, 1);
+  fi.pa = NQ_(qb, Q_P, 1); fi.pb = NQ_(qt, Q_P, 1);
+  fi.ta = NQ_(qb, Q_TCL, 1); fi.tb = NQ_(qt, Q_TCL, 1);
+  fi.ca = NQ_(qb, Q_CP, 1); fi.cb = NQ_(qt, Q_CP, 1);
+  fi.ka = NQ_(qb, Q_TCAP, 1); fi.kb = NQ_(qt, Q_TCAP, 1);
   const double rdy = a.rdy, q_rdx = 0.25 * a.rdx;
   fi.drn = rdy * (fi.rb - fi.ra);
-  fi.drt = 0.5 * (R.n(yb, Q_GX, pc) + R.n(yt, Q_GX, pc));
+  fi.drt = NQ_(qb, Q_GXH, 1) + NQ_(qt, Q_GXH, 1);
   fi.dunn = rdy * (fi.unb - fi.una);
-  fi.dunt = q_rdx * ((R.u(yb, 1, pc + 1) + R.u(yt, 1, pc + 1)) - (R.u(yb, 1, pc - 1) + R.u(yt, 1, pc - 1)));
+  fi.dunt = q_rdx * ((UV(ub, 1, 2) + UV(ut, 1, 2)) - (UV(ub, 1, 0) + UV(ut, 1, 0)));
   fi.dutn = rdy * (fi.utb - fi.uta);
-  fi.dutt = q_rdx * ((R.u(yb, 0, pc + 1) + R.u(yt, 0, pc + 1)) - (R.u(yb, 0, pc - 1) + R.u(yt, 0, pc - 1)));
-  fi.lap = 0.5 * (R.n(yb, Q_LAP, pc) + R.n(yt, Q_LAP, pc));
+  fi.dutt = q_rdx * ((UV(ub, 0, 2) + UV(ut, 0, 2)) - (UV(ub, 0, 0) + UV(ut, 0, 0)));
+  fi.lap = NQ_(qb, Q_LAPH, 1) + NQ_(qt, Q_LAPH, 1);
   fi.dtn = rdy * (fi.tb - fi.ta);
   fi.dkn = rdy * (fi.kb - fi.ka);
   double F[4];
   const bool s_face = WALL && a.wall_s && yt == BC;
   const bool n_face = WALL && a.wall_n && yt == a.f.ny - BC;
   if (s_face || n_face) {
-    const int row = s_face ? yt : yb;
-    const double tl = k.c38cv * (R.n(row, Q_TCL, pc) - k.iwe * R.n(row, Q_TCAP, pc));
+    const int qo = s_face ? qt : qb;
+    const double tl = k.c38cv * (NQ_(qo, Q_TCL, 1) - k.iwe * NQ_(qo, Q_TCAP, 1));
     const double q = wall_heat_flux(a.wall, a.xmap0 + x * a.dx);
     wall_face_flux(fi, tl, a.dy, q, s_face ? q : -q, k, F);
   } else {
@@ -222,10 +218,7 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost
     }
     b -= ghost_ctas;
   }
-  extern __shared__ __align__(16) double sm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* base = sm + warp * WARP_DOUBLES;
-  const Ring R{base, base + NS * 4 * RC, base + NS * 4 * RC + NUV * 2 * PC};
   const Field f = a.f;
   const int c0 = BC + (b % sx) * SW;
   const int y0 = BC + ((b / sx) * WPC + warp) * H;
@@ -233,32 +226,40 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost
   if (y0 > ylast) return;  // the whole warp leaves; no CTA barrier is used
   const int y1 = min(y0 + H, ylast + 1);
   const int x = c0 + lane;
-  const int xl = min(lane, SW), yl = min(lane, SW - 1);  // clamped face columns
   const DimConst& k = a.k;
-  const double hrdx = 0.5 * a.rdx, hrdy = 0.5 * a.rdy;
-  const double rdx2 = a.rdx * a.rdx, rdy2 = a.rdy * a.rdy;
+  const double qrdx = 0.25 * a.rdx, qrdy = 0.25 * a.rdy;
+  const double hrdx2 = 0.5 * a.rdx * a.rdx, hrdy2 = 0.5 * a.rdy * a.rdy;
 
-  // prologue: node quantities of rows y0-1 and y0, bottom face of row y0,
-  // state rows y0 .. y0+2 in the ring
+  // ring row offsets (warp base + lane column)
+  const int wb = warp * WARP_DOUBLES + lane;
+  int s0 = wb, s1 = wb + ST_ROW, s2 = wb + 2 * ST_ROW;  // state rows
+  const int ub = wb + NS * ST_ROW;
+  int um = ub, u0 = ub + UV_ROW, u1 = ub + 2 * UV_ROW;  // velocity rows
+  const int qbase = ub + NUV * UV_ROW;
+  int q0 = qbase, q1 = qbase + Q_ROW;                   // node rows
+
+  // prologue: node quantities of rows y0-1 (into um, q1) and y0 (into u0,
+  // q0), bottom face of row y0; then state rows y0 .. y0+2 in s0 .. s2
   double v[2][4];
-#pragma unroll 1
-  for (int row = y0 - 2; row <= y0; row++) {
-    load_row(a, c0, row, lane, v);
-    store_row(R, row, lane, v);
-  }
+  load_row(a, c0, y0 - 2, lane, v);
+  store_row(s1, lane, v);
+  load_row(a, c0, y0 - 1, lane, v);
+  store_row(s2, lane, v);
+  load_row(a, c0, y0, lane, v);
+  store_row(s0, lane, v);
   __syncwarp();
-  node_row(R, y0 - 1, lane, hrdx, hrdy, rdx2, rdy2, k);
+  node_row(s1, s2, s0, um, q1, qrdx, qrdy, hrdx2, hrdy2, k);
   load_row(a, c0, y0 + 1, lane, v);
   __syncwarp();  // state row y0-2 is no longer read
-  store_row(R, y0 + 1, lane, v);
+  store_row(s1, lane, v);
   __syncwarp();
-  node_row(R, y0, lane, hrdx, hrdy, rdx2, rdy2, k);
+  node_row(s2, s0, s1, u0, q0, qrdx, qrdy, hrdx2, hrdy2, k);
   __syncwarp();
   double Gb[4];
-  y_face<WALL>(a, R, yl, x, y0 - 1, Gb);
+  y_face<WALL>(a, s2, s0, um, u0, q1, q0, x, y0 - 1, Gb);
   load_row(a, c0, y0 + 2, lane, v);
   __syncwarp();  // state row y0-1 is no longer read
-  store_row(R, y0 + 2, lane, v);
+  store_row(s2, lane, v);
   __syncwarp();
 
   const bool active = lane < SW && x <= f.nx - 1 - BC;
@@ -269,15 +270,17 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost
     else if (x >= f.nx - 2 * BC) ix2 = x - px;
   }
 
+  // s0/s1/s2 = state rows y, y+1, y+2; um/u0 = velocity rows y-1, y and u1
+  // the free row; q0 = node row y and q1 the free row
 #pragma unroll 1
   for (int y = y0; y < y1; y++) {
     double nxt[2][4];
     load_row(a, c0, y + 3, lane, nxt);  // prefetch
-    node_row(R, y + 1, lane, hrdx, hrdy, rdx2, rdy2, k);
+    node_row(s0, s1, s2, u1, q1, qrdx, qrdy, hrdx2, hrdy2, k);
     __syncwarp();
     double Fx[4], Gt[4];
-    x_face<WALL>(a, R, xl, x, y, Fx);
-    y_face<WALL>(a, R, yl, x, y, Gt);
+    x_face<WALL>(a, s0, um, u0, u1, q0, x, Fx);
+    y_face<WALL>(a, s0, s1, u0, u1, q0, q1, x, y, Gt);
     double Fr[4];
 #pragma unroll
     for (int v = 0; v < 4; v++) Fr[v] = __shfl_down_sync(0xffffffffu, Fx[v], 1);
@@ -289,8 +292,7 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost
         if (y < 2 * BC) iy2 = y + py;
         else if (y >= f.ny - 2 * BC) iy2 = y - py;
       }
-      const double uc[4] = {R.r(y, 0, lane + 2), R.r(y, 1, lane + 2), R.r(y, 2, lane + 2),
-                            R.r(y, 3, lane + 2)};
+      const double uc[4] = {ST(s0, 0, 2), ST(s0, 1, 2), ST(s0, 2, 2), ST(s0, 3, 2)};
 #pragma unroll
       for (int v = 0; v < 4; v++) {
         double L = (Fx[v] - Fr[v]) * a.rdx + (Gb[v] - Gt[v]) * a.rdy;
@@ -316,10 +318,25 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost
 #pragma unroll
     for (int v = 0; v < 4; v++) Gb[v] = Gt[v];
     __syncwarp();  // state row y is no longer read
-    store_row(R, y + 3, lane, nxt);
+    store_row(s0, lane, nxt);  // row y+3 takes the slot of row y
     __syncwarp();
+    const int t = s0;
+    s0 = s1;
+    s1 = s2;
+    s2 = t;
+    const int tu = um;
+    um = u0;
+    u0 = u1;
+    u1 = tu;
+    const int tq = q0;
+    q0 = q1;
+    q1 = tq;
   }
 }
+
+#undef ST
+#undef UV
+#undef NQ_
 
 template <int H, int WPC, int MINB, int MODE>
 const void* strip_fn(int kind) {
