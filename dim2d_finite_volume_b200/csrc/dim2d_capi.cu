@@ -251,7 +251,7 @@ int dim2d_create(const dim2d_params* p, int nx, int ny, const int bc_choice[8],
 int dim2d_destroy(dim2d_handle* h) {
   if (!h) return DIM2D_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
-  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  drop_graphs(h);
   for (cudaEvent_t ev : h->prof_ev) cudaEventDestroy(ev);
   cudaFree(h->A);
   cudaFree(h->B);
@@ -293,9 +293,14 @@ int dim2d_upload(dim2d_handle* h, const double* nodes, const double* x_map, cons
                         h->stream);
   if (e != cudaSuccess) return cuda_error(e, "upload");
   // td_operators_class.f:157-158
-  h->dx = x_map[1] - x_map[0];
-  h->dy = y_map[1] - y_map[0];
-  if (!(h->dx > 0) || !(h->dy > 0)) return set_error(DIM2D_ERR_ARG, "upload: x_map/y_map not increasing");
+  const double dx = x_map[1] - x_map[0], dy = y_map[1] - y_map[0];
+  if (!(dx > 0) || !(dy > 0)) return set_error(DIM2D_ERR_ARG, "upload: x_map/y_map not increasing");
+  // captured step graphs hold dx, dy and the map origins as kernel
+  // parameters: keep them only while those are unchanged
+  if (!h->uploaded || dx != h->dx || dy != h->dy || x_map[0] != h->xmap0 || y_map[0] != h->ymap0)
+    h->graph_dt = -1.0;
+  h->dx = dx;
+  h->dy = dy;
   h->rdx = 1.0 / h->dx;
   h->rdy = 1.0 / h->dy;
   h->xmap0 = x_map[0];
@@ -306,7 +311,6 @@ int dim2d_upload(dim2d_handle* h, const double* nodes, const double* x_map, cons
   h->y_max = y_map[f.ny - 1 - BC];
   h->t = t;
   h->uploaded = true;
-  h->graph_dt = -1.0;  // invalidate captured step graphs
   return DIM2D_OK;
 }
 
@@ -337,6 +341,7 @@ int dim2d_set_variant(dim2d_handle* h, int variant) {
   if (variant < 0 || variant >= NUM_VARIANTS)
     return set_error(DIM2D_ERR_ARG, "set_variant: variant %d out of range", variant);
   h->variant = variant;
+  h->graph_dt = -1.0;  // the captured kernels belong to the previous variant
   return DIM2D_OK;
 }
 
@@ -392,6 +397,7 @@ int dim2d_autotune(dim2d_handle* h, int* chosen, double* times_ms) {
     return cuda_error(e, "autotune");
   }
   h->variant = best;
+  h->graph_dt = -1.0;
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     g_tune[key] = best;
@@ -471,10 +477,12 @@ int dim2d_step(dim2d_handle* h, double dt, int nsteps) {
   if (!h) return set_error(DIM2D_ERR_ARG, "step: null handle");
   if (!h->uploaded) return set_error(DIM2D_ERR_NOT_READY, "step: no state uploaded");
   if (nsteps < 0 || !std::isfinite(dt)) return set_error(DIM2D_ERR_ARG, "step: bad dt/nsteps");
-  for (int s = 0; s < nsteps; s++) {
-    int rc = rk3_step(h, dt);
-    if (rc) return rc;
-  }
+  return rk3_steps(h, dt, nsteps);
+}
+
+int dim2d_set_graphs(dim2d_handle* h, int enable) {
+  if (!h) return set_error(DIM2D_ERR_ARG, "set_graphs: null handle");
+  h->use_graphs = enable != 0;
   return DIM2D_OK;
 }
 

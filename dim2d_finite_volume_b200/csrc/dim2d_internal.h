@@ -40,9 +40,14 @@ struct dim2d_handle {
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
   long long launches = 0;
-  // captured two-step graph (A -> B -> A), valid for graph_dt
-  cudaGraphExec_t graph_exec = nullptr;
+  // captured one-step graphs, one per buffer parity (which buffer holds
+  // u^n); slot i is valid for graph_dt[i] and graph_A[i].  graph_dt = -1
+  // invalidates both (set by anything that changes kernel parameters).
+  bool use_graphs = true;
+  cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
   double graph_dt = -1.0;
+  const double* graph_A[2] = {nullptr, nullptr};
+  long long graph_launches[2] = {0, 0};  // kernel launches in one replay
   // live timing of the interior stage kernel (dim2d_profile)
   bool prof = false;
   std::vector<cudaEvent_t> prof_ev;  // start/stop pairs
@@ -72,6 +77,9 @@ WallConst make_wall(const dim2d_params& p);
 dim2d::StageArgs make_stage_args(const dim2d_handle* h, const double* uin, double* uout,
                                  double dt, int st);
 int rk3_step(dim2d_handle* h, double dt);
+// nsteps RK3 steps; each step replays a captured CUDA graph when graphs are
+// enabled and the handle is not profiling
+int rk3_steps(dim2d_handle* h, double dt, int nsteps);
 // the complete work of one stage (mode 1) or time derivative (mode 0): the
 // stage kernel and, on open fields where the stage kernel does not cover
 // them, the ghost-cell kernel; counts launches, profiles the stage kernel
@@ -81,3 +89,4 @@ int check_status(dim2d_handle* h);
 // bracket one launch with profiling events (no-op unless h->prof)
 void prof_begin(dim2d_handle* h);
 void prof_end(dim2d_handle* h);
+void drop_graphs(dim2d_handle* h);

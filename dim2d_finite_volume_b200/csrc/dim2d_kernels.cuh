@@ -1,5 +1,6 @@
 // dim2d_kernels.cuh -- launch interface of the sm_100a kernels.
 #pragma once
+#include <cstdint>
 #include <cuda_runtime.h>
 
 #include "dim2d_physics.cuh"
@@ -79,8 +80,16 @@ cudaError_t launch_interior_stage(const StageArgs& a, cudaStream_t s);
 // warp-streaming variant (dim2d_strip.cu); mode 0 = L(u), 1 = stage update;
 // shape 0..4 = strip height / warps per CTA (8,4) (16,4) (32,4) (16,8) (8,8)
 cudaError_t launch_strip_stage(const StageArgs& a, int mode, int shape, cudaStream_t s);
+// The strip kernels read state rows as 16-byte pairs: they need an even
+// pitch and 16-byte aligned input planes (fields allocated by the library
+// always qualify; caller-provided layouts may not, and then use variant 0).
+inline bool strip_layout_ok(const StageArgs& a) {
+  return a.f.pitch % 2 == 0 && reinterpret_cast<uintptr_t>(a.uin) % 16 == 0;
+}
+// 1 if the stage launch of `a` runs a strip kernel
+inline bool stage_uses_strip(const StageArgs& a) { return a.variant > 0 && strip_layout_ok(a); }
 // 1 if the stage launch of `a` also covers the open-boundary ghost cells
-inline bool stage_fuses_open(const StageArgs& a) { return a.open && a.variant > 0; }
+inline bool stage_fuses_open(const StageArgs& a) { return a.open && stage_uses_strip(a); }
 constexpr int NUM_VARIANTS = 6;
 // L(a.uin) of the interior cells into a.uout (stage fields ignored)
 cudaError_t launch_time_dev(const StageArgs& a, cudaStream_t s);

@@ -142,3 +142,84 @@ int rk3_step(dim2d_handle* h, double dt) {
   h->t += dt;  // field_class.f:70
   return DIM2D_OK;
 }
+
+void drop_graphs(dim2d_handle* h) {
+  for (int i = 0; i < 2; i++) {
+    if (h->graph_exec[i]) cudaGraphExecDestroy(h->graph_exec[i]);
+    h->graph_exec[i] = nullptr;
+    h->graph_A[i] = nullptr;
+  }
+}
+
+// Capture one RK3 step into graph slot `slot`.  The capture runs
+// rk3_step's host side (A/B swap, time += dt) without executing anything;
+// on success the caller launches the graph once, which brings the device
+// state to the host state.  On failure the host side is rolled back.  No
+// kernel reads the field time, so one graph serves every time level.
+static int capture_step(dim2d_handle* h, double dt, int slot) {
+  if (h->graph_exec[slot]) cudaGraphExecDestroy(h->graph_exec[slot]);
+  h->graph_exec[slot] = nullptr;
+  h->graph_A[slot] = nullptr;
+  double* const A0 = h->A;
+  double* const B0 = h->B;
+  const double t0 = h->t;
+  const long long n0 = h->launches;
+  cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return DIM2D_ERR_UNSUPPORTED;  // e.g. the legacy default stream
+  }
+  const int rc = rk3_step(h, dt);
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(h->stream, &g);
+  const long long n = h->launches - n0;
+  h->launches = n0;
+  cudaGraphExec_t x = nullptr;
+  if (!rc && e == cudaSuccess && g) e = cudaGraphInstantiate(&x, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (rc || e != cudaSuccess || !x) {
+    cudaGetLastError();
+    h->A = A0;
+    h->B = B0;
+    h->t = t0;
+    return rc ? rc : DIM2D_ERR_UNSUPPORTED;
+  }
+  h->graph_exec[slot] = x;
+  h->graph_A[slot] = A0;
+  h->graph_launches[slot] = n;
+  return DIM2D_OK;
+}
+
+int rk3_steps(dim2d_handle* h, double dt, int nsteps) {
+  const bool graphs = h->use_graphs && !h->prof;
+  if (graphs && h->graph_dt != dt) {
+    drop_graphs(h);
+    h->graph_dt = dt;
+  }
+  for (int s = 0; s < nsteps; s++) {
+    if (graphs) {
+      int slot = -1;
+      for (int i = 0; i < 2; i++)
+        if (h->graph_exec[i] && h->graph_A[i] == h->A) slot = i;
+      bool fresh = false;
+      if (slot < 0) {
+        slot = (h->graph_exec[0] && h->graph_A[0] != h->A) ? 1 : 0;
+        fresh = capture_step(h, dt, slot) == DIM2D_OK;
+        if (!fresh) slot = -1;
+      }
+      if (slot >= 0) {
+        cudaError_t e = cudaGraphLaunch(h->graph_exec[slot], h->stream);
+        if (e != cudaSuccess) return cuda_error(e, "step graph");
+        h->launches += h->graph_launches[slot];
+        if (!fresh) {  // the host side of rk3_step
+          std::swap(h->A, h->B);
+          h->t += dt;  // field_class.f:70
+        }
+        continue;
+      }
+    }
+    int rc = rk3_step(h, dt);
+    if (rc) return rc;
+  }
+  return DIM2D_OK;
+}

@@ -60,32 +60,30 @@ extern __shared__ __align__(16) double g_ring[];
 #define UV(o, c, dc) g_ring[(o) + (c) * PC + (dc)]
 #define NQ_(o, c, dc) g_ring[(o) + (c) * PC + (dc)]
 
-// global loads of the state row `row` for columns c0-2+lane and c0+30+lane
+// global loads of the state row `row` as 16-byte pairs: lane p < 17 reads
+// columns c0-2+2p and c0-1+2p of the 4 planes (lanes 17..31 repeat lane
+// 16).  Addresses are clamped to the field's rows and to its pitch, so no
+// load leaves the allocation; the clamped values land in ring columns that
+// only unused lanes read.  Needs an even pitch and 16-byte aligned planes
+// (strip_layout_ok).
 __device__ __forceinline__ void load_row(const StageArgs& a, int c0, int row, int lane,
-                                         double v[2][4]) {
-#pragma unroll
-  for (int s = 0; s < 2; s++) {
-    const int col = lane + 32 * s;
-    const int x = c0 - 2 + col;
-    v[s][0] = 1.0;  // benign values past the field edge
-    v[s][1] = v[s][2] = v[s][3] = 0.0;
-    if (col < RC && x < a.f.nx && row < a.f.ny) {
-      const size_t o = (size_t)row * a.f.pitch + x;
-      v[s][0] = __ldg(a.uin + o);
-      v[s][1] = __ldg(a.uin + o + a.f.plane);
-      v[s][2] = __ldg(a.uin + o + 2 * a.f.plane);
-      v[s][3] = __ldg(a.uin + o + 3 * a.f.plane);
-    }
-  }
+                                         double2 v[4]) {
+  const int r = min(row, a.f.ny - 1);
+  const int xp = min(c0 - 2 + 2 * min(lane, 16), a.f.pitch - 2);
+  const double2* p = reinterpret_cast<const double2*>(a.uin + (size_t)r * a.f.pitch + xp);
+  const size_t pl = a.f.plane / 2;
+  v[0] = __ldg(p);
+  v[1] = __ldg(p + pl);
+  v[2] = __ldg(p + 2 * pl);
+  v[3] = __ldg(p + 3 * pl);
 }
 
-// state row into the ring row at offset o (lane's column 0 = c0-2+lane)
-__device__ __forceinline__ void store_row(int o, int lane, const double v[2][4]) {
+// state row into the ring row at offset o (which includes the lane)
+__device__ __forceinline__ void store_row(int o, int lane, const double2 v[4]) {
+  if (lane < 17) {
+    double2* d = reinterpret_cast<double2*>(g_ring + (o - lane) + 2 * lane);
 #pragma unroll
-  for (int q = 0; q < 4; q++) ST(o, q, 0) = v[0][q];
-  if (lane + 32 < RC) {
-#pragma unroll
-    for (int q = 0; q < 4; q++) ST(o, q, 32) = v[1][q];
+    for (int q = 0; q < 4; q++) d[q * (RC / 2)] = v[q];
   }
 }
 
@@ -240,7 +238,7 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost
 
   // prologue: node quantities of rows y0-1 (into um, q1) and y0 (into u0,
   // q0), bottom face of row y0; then state rows y0 .. y0+2 in s0 .. s2
-  double v[2][4];
+  double2 v[4];
   load_row(a, c0, y0 - 2, lane, v);
   store_row(s1, lane, v);
   load_row(a, c0, y0 - 1, lane, v);
@@ -274,7 +272,7 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost
   // the free row; q0 = node row y and q1 the free row
 #pragma unroll 1
   for (int y = y0; y < y1; y++) {
-    double nxt[2][4];
+    double2 nxt[4];
     load_row(a, c0, y + 3, lane, nxt);  // prefetch
     node_row(s0, s1, s2, u1, q1, qrdx, qrdy, hrdx2, hrdy2, k);
     __syncwarp();
@@ -284,15 +282,12 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost
     double Fr[4];
 #pragma unroll
     for (int v = 0; v < 4; v++) Fr[v] = __shfl_down_sync(0xffffffffu, Fx[v], 1);
-    if (active) {
-      const size_t go = (size_t)y * f.pitch + x;
-      int iy2 = -1;
-      if (a.periodic) {
-        const int py = f.ny - 2 * BC;
-        if (y < 2 * BC) iy2 = y + py;
-        else if (y >= f.ny - 2 * BC) iy2 = y - py;
-      }
+    {
+      // every lane evaluates the update (clamped column for its loads);
+      // only active lanes store
+      const size_t go = (size_t)y * f.pitch + min(x, f.nx - 1 - BC);
       const double uc[4] = {ST(s0, 0, 2), ST(s0, 1, 2), ST(s0, 2, 2), ST(s0, 3, 2)};
+      double out[4];
 #pragma unroll
       for (int v = 0; v < 4; v++) {
         double L = (Fx[v] - Fr[v]) * a.rdx + (Gb[v] - Gt[v]) * a.rdy;
@@ -300,17 +295,26 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost
           if (v == 2) L += -uc[0] * k.gravity;
           if (v == 3) L += -uc[2] * k.gravity;
         }
-        double out;
-        if (MODE == 0) out = L;
-        else if (a.stage == 1) out = uc[v] + a.dt * L;
-        else out = a.b * __ldg(a.u0 + go + v * f.plane) + (1.0 - a.b) * (uc[v] + a.dt * L);
-        double* dst = a.uout + v * f.plane;
-        dst[go] = out;
+        if (MODE == 0) out[v] = L;
+        else if (a.stage == 1) out[v] = uc[v] + a.dt * L;
+        else out[v] = a.b * __ldg(a.u0 + go + v * f.plane) + (1.0 - a.b) * (uc[v] + a.dt * L);
+      }
+      if (active) {
+#pragma unroll
+        for (int v = 0; v < 4; v++) a.uout[go + v * f.plane] = out[v];
         if (MODE == 1 && a.periodic) {  // periodic_xy/bc_operators_class.f:156-199
-          if (ix2 >= 0) dst[(size_t)y * f.pitch + ix2] = out;
-          if (iy2 >= 0) {
-            dst[(size_t)iy2 * f.pitch + x] = out;
-            if (ix2 >= 0) dst[(size_t)iy2 * f.pitch + ix2] = out;
+          int iy2 = -1;
+          const int py = f.ny - 2 * BC;
+          if (y < 2 * BC) iy2 = y + py;
+          else if (y >= f.ny - 2 * BC) iy2 = y - py;
+#pragma unroll
+          for (int v = 0; v < 4; v++) {
+            double* dst = a.uout + v * f.plane;
+            if (ix2 >= 0) dst[(size_t)y * f.pitch + ix2] = out[v];
+            if (iy2 >= 0) {
+              dst[(size_t)iy2 * f.pitch + x] = out[v];
+              if (ix2 >= 0) dst[(size_t)iy2 * f.pitch + ix2] = out[v];
+            }
           }
         }
       }
@@ -371,7 +375,7 @@ cudaError_t launch_strip_stage(const StageArgs& a, int mode, int shape, cudaStre
     case 0: return launch_strip_shape<8, 4, 4>(a, mode, s);
     case 1: return launch_strip_shape<16, 4, 4>(a, mode, s);
     case 2: return launch_strip_shape<16, 4, 5>(a, mode, s);
-    case 3: return launch_strip_shape<8, 4, 5>(a, mode, s);
+    case 3: return launch_strip_shape<16, 2, 8>(a, mode, s);
     case 4: return launch_strip_shape<16, 8, 2>(a, mode, s);
   }
   return cudaErrorInvalidValue;

@@ -135,6 +135,7 @@ def library():
         "dim2d_profile_read": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_double),
                                               ctypes.POINTER(ctypes.c_longlong)]),
         "dim2d_set_variant": (ctypes.c_int, [H, ctypes.c_int]),
+        "dim2d_set_graphs": (ctypes.c_int, [H, ctypes.c_int]),
         "dim2d_get_variant": (ctypes.c_int, [H]),
         "dim2d_autotune": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_int), _dp]),
         "dim2d_destroy": (ctypes.c_int, [H]),
@@ -278,6 +279,10 @@ class Field:
     @variant.setter
     def variant(self, v):
         _check(library().dim2d_set_variant(self._h, int(v)))
+
+    def set_graphs(self, enable):
+        """Replay pairs of steps from a captured CUDA graph (default on)."""
+        _check(library().dim2d_set_graphs(self._h, 1 if enable else 0))
 
     def autotune(self, measure=False):
         """Time every stage-kernel variant on the resident field and keep

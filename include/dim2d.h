@@ -132,8 +132,14 @@ DIM2D_API int dim2d_upload(dim2d_handle *h, const double *nodes, const double *x
 
 /* nsteps calls of field%integrate(dt): three RK3-TVD stages each with
  * compute_time_dev, the stage update and apply_bc_on_nodes
- * (td_integrator_class.f:103-161, rk3tvd_steps_module.f:52-490), time += dt. */
+ * (td_integrator_class.f:103-161, rk3tvd_steps_module.f:52-490), time += dt.
+ * Each step replays a CUDA graph captured on first use for this dt (one
+ * per buffer parity; not while profiling or when disabled with
+ * dim2d_set_graphs); launches and results are those of the stream path. */
 DIM2D_API int dim2d_step(dim2d_handle *h, double dt, int nsteps);
+/* No counterpart in the reference.  Enable (default) or disable the step
+ * graphs of dim2d_step. */
+DIM2D_API int dim2d_set_graphs(dim2d_handle *h, int enable);
 
 /* time_dev(nx,ny,4) = L(nodes) of the resident state, interior cells (and
  * the ghost cells of time-derivative boundaries); other cells are written
@@ -170,7 +176,7 @@ DIM2D_API int dim2d_profile_read(dim2d_handle *h, double *ms, long long *launche
 /* No counterpart in the reference (its stage loops have one fixed shape).
  * Stage-kernel variant: 0 = 32x8-cell CTA tiles; 1..5 = warp-streaming
  * strips 30 columns wide with (rows per warp, warps per CTA, resident CTAs
- * per SM) = (8,4,4), (16,4,4), (16,4,5), (8,4,5), (16,8,2).  Every variant
+ * per SM) = (8,4,4), (16,4,4), (16,4,5), (16,2,8), (16,8,2).  Every variant
  * evaluates the same face fluxes; results agree to rounding. */
 #define DIM2D_NUM_VARIANTS 6
 DIM2D_API int dim2d_set_variant(dim2d_handle *h, int variant);
