@@ -274,6 +274,14 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost
   for (int y = y0; y < y1; y++) {
     double2 nxt[4];
     load_row(a, c0, y + 3, lane, nxt);  // prefetch
+    // u^n of this row's cells (stages 2 and 3), issued before the node and
+    // face work so its latency is hidden; clamped column for unused lanes
+    const size_t go = (size_t)y * f.pitch + min(x, f.nx - 1 - BC);
+    double un[4] = {0.0, 0.0, 0.0, 0.0};
+    if (MODE == 1 && a.stage != 1) {
+#pragma unroll
+      for (int v = 0; v < 4; v++) un[v] = __ldg(a.u0 + go + v * f.plane);
+    }
     node_row(s0, s1, s2, u1, q1, qrdx, qrdy, hrdx2, hrdy2, k);
     __syncwarp();
     double Fx[4], Gt[4];
@@ -283,9 +291,7 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost
 #pragma unroll
     for (int v = 0; v < 4; v++) Fr[v] = __shfl_down_sync(0xffffffffu, Fx[v], 1);
     {
-      // every lane evaluates the update (clamped column for its loads);
-      // only active lanes store
-      const size_t go = (size_t)y * f.pitch + min(x, f.nx - 1 - BC);
+      // every lane evaluates the update; only active lanes store
       const double uc[4] = {ST(s0, 0, 2), ST(s0, 1, 2), ST(s0, 2, 2), ST(s0, 3, 2)};
       double out[4];
 #pragma unroll
@@ -297,7 +303,7 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost
         }
         if (MODE == 0) out[v] = L;
         else if (a.stage == 1) out[v] = uc[v] + a.dt * L;
-        else out[v] = a.b * __ldg(a.u0 + go + v * f.plane) + (1.0 - a.b) * (uc[v] + a.dt * L);
+        else out[v] = a.b * un[v] + (1.0 - a.b) * (uc[v] + a.dt * L);
       }
       if (active) {
 #pragma unroll

@@ -181,11 +181,12 @@ DIM2D_API int dim2d_profile_read(dim2d_handle *h, double *ms, long long *launche
 #define DIM2D_NUM_VARIANTS 6
 DIM2D_API int dim2d_set_variant(dim2d_handle *h, int variant);
 DIM2D_API int dim2d_get_variant(const dim2d_handle *h);
-/* Autotuner: times every variant on the resident field (time-derivative
- * launches; the state is not modified), selects the fastest and caches the
- * choice for fields of the same size and boundary class in this process.
- * times_ms (optional, DIM2D_NUM_VARIANTS entries) receives the average
- * launch time of each variant; passing it forces a new measurement. */
+/* Autotuner: times every variant on the resident field (dry RK3 steps with
+ * dt = 0 that write only the two stage buffers; the state is not
+ * modified), selects the fastest and caches the choice for fields of the
+ * same size and boundary class in this process.  times_ms (optional,
+ * DIM2D_NUM_VARIANTS entries) receives the average dry-step time of each
+ * variant; passing it forces a new measurement. */
 DIM2D_API int dim2d_autotune(dim2d_handle *h, int *chosen, double *times_ms);
 
 DIM2D_API int dim2d_destroy(dim2d_handle *h);
