@@ -250,6 +250,7 @@ int dim2d_create(const dim2d_params* p, int nx, int ny, const int bc_choice[8],
 
 int dim2d_destroy(dim2d_handle* h) {
   if (!h) return DIM2D_OK;
+  if (h->batch) dim2d_batch_remove(h->batch, h);
   if (h->stream) cudaStreamSynchronize(h->stream);
   drop_graphs(h);
   for (cudaEvent_t ev : h->prof_ev) cudaEventDestroy(ev);
@@ -488,6 +489,7 @@ int dim2d_step(dim2d_handle* h, double dt, int nsteps) {
   if (!h) return set_error(DIM2D_ERR_ARG, "step: null handle");
   if (!h->uploaded) return set_error(DIM2D_ERR_NOT_READY, "step: no state uploaded");
   if (nsteps < 0 || !std::isfinite(dt)) return set_error(DIM2D_ERR_ARG, "step: bad dt/nsteps");
+  if (h->batch) return set_error(DIM2D_ERR_ARG, "step: the field is advanced by its batch");
   return rk3_steps(h, dt, nsteps);
 }
 

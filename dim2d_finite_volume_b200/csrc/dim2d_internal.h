@@ -22,6 +22,7 @@ struct dim2d_handle {
   unsigned int* status = nullptr;  // wall root status word (device)
   double xmap0 = 0, ymap0 = 0;     // x_map(1), y_map(1)
   int variant = 0;                 // stage-kernel variant (dim2d_set_variant)
+  struct dim2d_batch* batch = nullptr;  // batch this field belongs to, if any
   int bc_choice[8]{}, bc_type[8]{}, bc_order[8]{};
   int side_kind[8]{};
   dim2d::Field f{};

@@ -101,4 +101,56 @@ cudaError_t launch_periodic_ghosts(double* u, const Field& f, cudaStream_t s);
 cudaError_t launch_cfl_max(const double* u, const Field& f, const DimConst& k, double* out,
                            cudaStream_t s);
 
+// ---- batched launches (dim2d_batch.cu): many fields of one boundary kind
+// advanced by one launch per stage.  The per-domain tables travel as
+// kernel parameters (read in place through __grid_constant__).
+constexpr int BATCH_MAX = 64;  // domains per launch (larger groups are split)
+
+struct BatchDomain {
+  Field f;
+  const double* uin;
+  const double* u0;
+  double* uout;
+  double dx, dy, rdx, rdy, dt, xmap0;
+  int periodic, wall_s;
+  int ghost0, strip0, sx;  // first ghost CTA, first strip CTA, strips per row
+};
+
+struct BatchStageArgs {
+  DimConst k;
+  WallConst wall;
+  int stage;
+  double b;
+  int ndom;
+  int ghost_ctas;  // total ghost CTAs (open kind), placed before all strips
+  BatchDomain d[BATCH_MAX];
+};
+
+// boundary kinds of a batched stage launch
+enum BatchKind : int { BK_PLAIN = 0, BK_WALL = 1, BK_OPEN = 2 };
+
+// one stage of every domain in P (shape as launch_strip_stage); fills the
+// CTA geometry fields of P.d
+cudaError_t launch_strip_batch(BatchStageArgs& P, int kind, int shape, cudaStream_t s);
+
+struct NodeBcDomain {
+  const double* utmp;
+  double* u;
+  Field f;
+  double dx, dy, rdx, rdy, xmap0, ymap0;
+  int south_wall, corners_y;
+  unsigned int* status;
+  int cta0;
+};
+
+struct NodeBcBatchArgs {
+  DimConst k;
+  WallConst wall;
+  int ndom;
+  NodeBcDomain d[BATCH_MAX];
+};
+
+// node boundary pass of every domain in P; fills P.d[].cta0
+cudaError_t launch_node_bc_batch(NodeBcBatchArgs& P, cudaStream_t s);
+
 }  // namespace dim2d

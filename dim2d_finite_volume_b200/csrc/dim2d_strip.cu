@@ -205,17 +205,9 @@ __device__ __forceinline__ void y_face(const StageArgs& a, int sb, int st, int u
 enum StripKind : int { K_PLAIN = 0, K_WALL = 1, K_OPEN = 2 };
 
 // grid: [ghost CTAs (K_OPEN only)] + sx * sy strip CTAs, x fastest
-template <int H, int WPC, int MINB, int MODE, int KIND>
-__global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost_ctas, int sx) {
-  constexpr bool WALL = KIND == K_WALL;
-  int b = blockIdx.x;
-  if (KIND == K_OPEN) {
-    if (b < ghost_ctas) {
-      open_ghost_cell(a, b * (32 * WPC) + threadIdx.x, MODE);
-      return;
-    }
-    b -= ghost_ctas;
-  }
+// The work of strip CTA number b of one field (sx strips per row band).
+template <int H, int WPC, int MODE, bool WALL>
+__device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const Field f = a.f;
   const int c0 = BC + (b % sx) * SW;
@@ -344,6 +336,80 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost
   }
 }
 
+template <int H, int WPC, int MINB, int MODE, int KIND>
+__global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost_ctas, int sx) {
+  int b = blockIdx.x;
+  if (KIND == K_OPEN) {
+    if (b < ghost_ctas) {
+      open_ghost_cell(a, b * (32 * WPC) + threadIdx.x, MODE);
+      return;
+    }
+    b -= ghost_ctas;
+  }
+  strip_cta<H, WPC, MODE, KIND == K_WALL>(a, b, sx);
+}
+
+// stage arguments of domain i of a batched launch
+__device__ __forceinline__ StageArgs batch_stage_args(const BatchStageArgs& P, int i) {
+  const BatchDomain& d = P.d[i];
+  StageArgs a;
+  a.uin = d.uin;
+  a.u0 = d.u0;
+  a.uout = d.uout;
+  a.f = d.f;
+  a.dx = d.dx;
+  a.dy = d.dy;
+  a.rdx = d.rdx;
+  a.rdy = d.rdy;
+  a.dt = d.dt;
+  a.b = P.b;
+  a.stage = P.stage;
+  a.periodic = d.periodic;
+  a.wall_w = a.wall_e = a.wall_n = 0;
+  a.wall_s = d.wall_s;
+  a.variant = 0;
+  a.open = 0;
+  a.t = 0.0;
+  a.xmap0 = d.xmap0;
+  a.ymap0 = 0.0;
+  a.wall = P.wall;
+  a.k = P.k;
+  return a;
+}
+
+// last domain i in [0, n) whose first CTA (ghost0 or strip0) is <= b
+template <bool GHOST>
+__device__ __forceinline__ int batch_domain(const BatchStageArgs& P, int b) {
+  int lo = 0, hi = P.ndom - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const int first = GHOST ? P.d[mid].ghost0 : P.d[mid].strip0;
+    if (first <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// One RK stage of every domain of a batch (one boundary kind): the ghost
+// CTAs of all domains first (open kind), then every domain's strip CTAs.
+template <int H, int WPC, int MINB, int KIND>
+__global__ void __launch_bounds__(32 * WPC, MINB)
+    k_strip_batch(const __grid_constant__ BatchStageArgs P) {
+  int b = blockIdx.x;
+  if (KIND == K_OPEN) {
+    if (b < P.ghost_ctas) {
+      const int i = batch_domain<true>(P, b);
+      const StageArgs a = batch_stage_args(P, i);
+      open_ghost_cell(a, (b - P.d[i].ghost0) * (32 * WPC) + threadIdx.x, 1);
+      return;
+    }
+    b -= P.ghost_ctas;
+  }
+  const int i = batch_domain<false>(P, b);
+  const StageArgs a = batch_stage_args(P, i);
+  strip_cta<H, WPC, 1, KIND == K_WALL>(a, b - P.d[i].strip0, P.d[i].sx);
+}
+
 #undef ST
 #undef UV
 #undef NQ_
@@ -372,7 +438,44 @@ cudaError_t launch_strip_shape(const StageArgs& a, int mode, cudaStream_t s) {
   return cudaLaunchKernel(fn, dim3(blocks), dim3(32 * WPC), args, smem, s);
 }
 
+template <int H, int WPC, int MINB>
+cudaError_t launch_strip_batch_shape(BatchStageArgs& P, int kind, cudaStream_t s) {
+  const size_t smem = (size_t)WPC * WARP_DOUBLES * sizeof(double);
+  const void* fn = kind == BK_WALL   ? (const void*)k_strip_batch<H, WPC, MINB, K_WALL>
+                   : kind == BK_OPEN ? (const void*)k_strip_batch<H, WPC, MINB, K_OPEN>
+                                     : (const void*)k_strip_batch<H, WPC, MINB, K_PLAIN>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  long long ghost = 0, strips = 0;
+  for (int i = 0; i < P.ndom; i++) {
+    BatchDomain& d = P.d[i];
+    d.sx = (d.f.nx - 2 * BC + SW - 1) / SW;
+    const int sy = (d.f.ny - 2 * BC + H * WPC - 1) / (H * WPC);
+    d.ghost0 = (int)ghost;
+    d.strip0 = (int)strips;
+    if (kind == BK_OPEN) ghost += (open_ghost_count(d.f) + 32 * WPC - 1) / (32 * WPC);
+    strips += (long long)d.sx * sy;
+  }
+  if (ghost + strips > 0x7fffffffLL) return cudaErrorInvalidValue;
+  P.ghost_ctas = (int)ghost;
+  void* args[] = {&P};
+  return cudaLaunchKernel(fn, dim3((unsigned)(ghost + strips)), dim3(32 * WPC), args, smem, s);
+}
+
 }  // namespace
+
+cudaError_t launch_strip_batch(BatchStageArgs& P, int kind, int shape, cudaStream_t s) {
+  if (P.ndom <= 0) return cudaSuccess;
+  if (P.ndom > BATCH_MAX) return cudaErrorInvalidValue;
+  switch (shape) {
+    case 0: return launch_strip_batch_shape<8, 4, 4>(P, kind, s);
+    case 1: return launch_strip_batch_shape<16, 4, 4>(P, kind, s);
+    case 2: return launch_strip_batch_shape<16, 4, 5>(P, kind, s);
+    case 3: return launch_strip_batch_shape<16, 2, 8>(P, kind, s);
+    case 4: return launch_strip_batch_shape<16, 8, 2>(P, kind, s);
+  }
+  return cudaErrorInvalidValue;
+}
 
 // shape id -> (rows per warp, warps per CTA, minimum resident CTAs per SM
 // requested from the register allocator)

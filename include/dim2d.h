@@ -214,6 +214,42 @@ DIM2D_API int dim2d_step_noalloc(const dim2d_params *p, int nx, int ny, const in
                                  const double *x_map, const double *y_map, double dt,
                                  int nsteps, void *stream);
 
+/* ---- Batches: no counterpart in the reference (one field per process
+ * there).  A batch advances many fields together: one launch per RK stage
+ * per boundary kind covers all its fields, and a step is a captured CUDA
+ * graph with one independent chain per kind (periodic_xy, hedstrom_xy,
+ * wall_S_reflection, reflection_xy), so the kinds overlap on the device.
+ * Members are fields created with dim2d_create and uploaded, on the
+ * batch's device, FP64, sharing one dim2d_params; the batch borrows their
+ * buffers and advances their state and time.  While a field is a member,
+ * dim2d_step on it is refused; dim2d_download/dim2d_time_dev of a member
+ * are ordered after the batch's queued steps.  dim2d_destroy of a member
+ * removes it first. */
+typedef struct dim2d_batch dim2d_batch;
+#define DIM2D_BATCH_GROUPS 4 /* periodic, open, wall_S, reflection */
+DIM2D_API int dim2d_batch_create(dim2d_batch **out);
+/* add a field that advances by dt per step */
+DIM2D_API int dim2d_batch_add(dim2d_batch *b, dim2d_handle *h, double dt);
+DIM2D_API int dim2d_batch_remove(dim2d_batch *b, dim2d_handle *h);
+DIM2D_API int dim2d_batch_set_dt(dim2d_batch *b, dim2d_handle *h, double dt);
+/* nsteps RK3 steps of every member (graph replays unless disabled) */
+DIM2D_API int dim2d_batch_step(dim2d_batch *b, int nsteps);
+/* wait for the batch and check the members' wall status words */
+DIM2D_API int dim2d_batch_sync(dim2d_batch *b);
+/* strip shape (0..4 = dim2d_set_variant 1..5) of one group */
+DIM2D_API int dim2d_batch_set_shape(dim2d_batch *b, int group, int shape);
+DIM2D_API int dim2d_batch_set_graphs(dim2d_batch *b, int enable);
+/* Autotuner: times dry steps (dt = 0, stage buffers only) of each group
+ * for the 5 strip shapes and keeps the fastest; chosen[4] receives the
+ * shapes, times_ms (optional) 4 x 5 dry-step times (0 for empty groups). */
+DIM2D_API int dim2d_batch_autotune(dim2d_batch *b, int chosen[4], double *times_ms);
+DIM2D_API int dim2d_batch_size(const dim2d_batch *b);
+DIM2D_API long long dim2d_batch_launch_count(const dim2d_batch *b);
+/* interior cells of all members (cell-updates per batch step) */
+DIM2D_API long long dim2d_batch_cells(const dim2d_batch *b);
+DIM2D_API int dim2d_batch_set_stream(dim2d_batch *b, void *stream);
+DIM2D_API int dim2d_batch_destroy(dim2d_batch *b);
+
 /* field_abstract_class.f:286-315: dx = (x_max-x_min)/(nx-1-2*bc_size). */
 DIM2D_API int dim2d_ini_coordinates(int nx, int ny, double x_min, double x_max, double y_min,
                           double y_max, double *x_map, double *y_map);

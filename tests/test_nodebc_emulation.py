@@ -25,7 +25,8 @@ def emu():
         pytest.skip("nvcc not available")
     d = tempfile.mkdtemp()
     exe = os.path.join(d, "emu_nodebc")
-    subprocess.check_call([NVCC, "-std=c++17", "-O1", "-w", "-I", os.path.join(ROOT, "include"),
+    subprocess.check_call([NVCC, "-std=c++17", "-O1", "-w", "-gencode", "arch=compute_100a,code=sm_100a",
+                           "-I", os.path.join(ROOT, "include"),
                            "-o", exe, os.path.join(HERE, "emu", "emu_nodebc.cu")])
     yield exe, d
     shutil.rmtree(d, ignore_errors=True)
