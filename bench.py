@@ -49,39 +49,21 @@ def parse():
     ap.add_argument("--bc", default="hedstrom_xy", choices=["hedstrom_xy", "periodic_xy"])
     ap.add_argument("--variant", default="auto",
                     help="stage-kernel variant 0..5, or 'auto' (the library's autotuner)")
+    ap.add_argument("--batch-domains", type=int, default=64,
+                    help="domains of the batched workload (0: skip it)")
     ap.add_argument("--cpu-budget", type=float, default=15.0,
                     help="seconds of host time for the cpu_baseline sample")
     return ap.parse_args()
 
 
 def workload(n, seed, rank=0, bc="hedstrom_xy"):
-    """The 1024^2 plain FP64 configuration: a bubble of seeded radius in
-    [0.05, 0.15] at T0 = 0.95, carried by a uniform x-flow at Mach 0.1 of
-    the liquid sound speed, open (Hedstrom) boundaries on all sides.
-    With bc='periodic_xy' the same bubble sits still in a periodic box."""
-    from dim2d_finite_volume_b200 import ic
-    rng = np.random.default_rng(seed + rank)
-    nx, ny, x_map, y_map = ic.grid(n)
-    dx = x_map[1] - x_map[0]
-    r = float(rng.uniform(0.05, 0.15))
-    T0 = 0.95
-    u0 = 0.0
-    if bc == "hedstrom_xy":
-        rv, rl = ic.maxwell_densities(T0)
-        e = rl * (8.0 / 3.0 * 2.5 * T0 - 3.0 * rl)
-        u0 = 0.1 * float(ic.sound_speed(np.array(rl), np.array(0.0), np.array(0.0),
-                                        np.array(e), 2.5))
-    q = ic.bubbles(x_map, y_map, T0, [(0.0, 0.0, r)], li=4.0 * dx, velocity=(u0, 0.0))
-    if bc == "periodic_xy":  # periodic ghosts as field%ini leaves them
-        px, py = nx - 4, ny - 4
-        q[:, :, 0:2] = q[:, :, px:px + 2]
-        q[:, :, nx - 2:] = q[:, :, 2:4]
-        q[:, 0:2, :] = q[:, py:py + 2, :]
-        q[:, ny - 2:, :] = q[:, 2:4, :]
-    rho_min = float(q[0].min())
-    dt = min(ic.cfl_dt(q, dx, dx, 0.1), 0.2 * 5.0 * rho_min * dx * dx)
-    return dict(nx=nx, ny=ny, x_map=x_map, y_map=y_map, nodes=np.ascontiguousarray(q), dt=dt,
-                radius=r, u0=u0, bc=bc)
+    """The 1024^2 plain FP64 configuration (workloads.plain_1024): a bubble
+    of seeded radius in [0.05, 0.15] at T0 = 0.95, carried by a uniform
+    x-flow at Mach 0.1 of the liquid sound speed, open (Hedstrom)
+    boundaries on all sides.  With bc='periodic_xy' the same bubble sits
+    still in a periodic box."""
+    from dim2d_finite_volume_b200 import workloads
+    return workloads.plain_1024(seed + rank, n, bc)
 
 
 def oracle_cfg(O, bc, nx, ny):
@@ -236,6 +218,71 @@ def run_reference(a, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(a, stream, barrier, F, torch, flush):
+    """Batched FP64 (64 seeded domains, n in {128..512}^2, wall / periodic /
+    open mix): the batch advanced by graph-replayed batched steps, against
+    the same fields stepped one field per launch.  Returns a dict."""
+    from dim2d_finite_volume_b200 import batch as Bm
+    from dim2d_finite_volume_b200 import workloads
+    doms = workloads.batched_domains(a.seed + 77, count=a.batch_domains)
+    fields = []
+    for d in doms:
+        fld = F.Field(d["nx"], d["ny"], bc=d["bc"])
+        fld.set_stream(stream.cuda_stream)
+        fld.ini(d["nodes"], d["x_map"], d["y_map"])
+        if d["bc"] not in ("periodic_xy", "hedstrom_xy"):
+            fld.apply_bc_on_nodes()  # field%ini
+        fields.append(fld)
+    # plain form first: each field its own launches (its step graph)
+    for fld in fields:
+        fld.variant = 2
+    for _ in range(3):
+        for fld, d in zip(fields, doms):
+            fld.integrate(d["dt"], 1)
+    barrier()
+    steps = max(3, a.steps // 2)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    plain_ms = 0.0
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.fill_(float(k))
+            e0.record(stream)
+            for fld, d in zip(fields, doms):
+                fld.integrate(d["dt"], 1)
+            e1.record(stream)
+            e1.synchronize()
+            plain_ms += e0.elapsed_time(e1)
+    barrier()
+    bt = Bm.Batch()
+    bt.set_stream(stream.cuda_stream)
+    for fld, d in zip(fields, doms):
+        bt.add(fld, d["dt"])
+    shapes, _ = bt.autotune()
+    cells = bt.cells
+    bt.step(3)
+    barrier()
+    n0 = bt.launches
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(a.steps)]
+    with torch.cuda.stream(stream):
+        for k in range(a.steps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            bt.step(1)
+            ev[k][1].record(stream)
+    barrier()
+    bt.sync()
+    launches = bt.launches - n0
+    batch_ms = sum(x.elapsed_time(y) for x, y in ev)
+    bt.close()
+    for fld in fields:
+        fld.close()
+    kinds = {k: sum(1 for d in doms if d["bc"] == k) for k in workloads.BATCH_KINDS}
+    return {"cells_per_step": int(cells), "steps": a.steps, "batch_ms": batch_ms,
+            "plain_ms": plain_ms, "plain_steps": steps, "launches": int(launches),
+            "domains": len(doms), "kinds": kinds, "shapes": shapes}
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -330,11 +377,39 @@ def main():
     e2e_ms = e0.elapsed_time(e1)
     clocks = sampler.stop()
     fld.close()
+    bres = None
+    if a.batch_domains > 0:
+        bres = run_batched(a, stream, barrier, F, torch, flush)
 
     t = torch.tensor([step_ms, e2e_ms], dtype=torch.float64, device="cuda")
     if dist is not None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     step_ms, e2e_ms = float(t[0]), float(t[1])
+    batched = None
+    if bres is not None:
+        tb = torch.tensor([bres["batch_ms"], bres["plain_ms"]], dtype=torch.float64, device="cuda")
+        if dist is not None:
+            dist.all_reduce(tb, op=dist.ReduceOp.MAX)
+        bv = bres["cells_per_step"] * world * bres["steps"] / (float(tb[0]) * 1e-3)
+        pv = bres["cells_per_step"] * world * bres["plain_steps"] / (float(tb[1]) * 1e-3)
+        peak_b, _ = measured_peaks()
+        batched = {
+            "workload": "batched FP64: %d seeded domains, n in {128,...,512}^2, T0 in "
+                        "[0.90,0.99], r in [0.05,0.2], wall (wall_S_reflection) / periodic / "
+                        "open mix, Mach in [0,0.1] on open domains" % bres["domains"],
+            "value": bv, "unit": "cell-updates/s", "ms_per_step": float(tb[0]) / bres["steps"],
+            "steps": bres["steps"], "cells_per_step": bres["cells_per_step"],
+            "kinds": bres["kinds"], "shapes": bres["shapes"],
+            "gpu_launches": bres["launches"],
+            "plain_per_field_value": pv,
+            "vs_plain_per_field": bv / pv,
+            "roofline": {"bound": "hbm", "achieved": bv * BYTES_PER_CELL_UPDATE / 1e9,
+                         "peak": peak_b, "unit": "GB/s",
+                         "frac": bv * BYTES_PER_CELL_UPDATE / 1e9 / peak_b},
+            "timing": "CUDA events around each batched step (one replay of the batch's step "
+                      "graph); plain: the same fields stepped one after another, each by its "
+                      "own step graph; L2 flushed between steps",
+        }
     total_cells = cells * world
     value = total_cells * a.steps / (step_ms * 1e-3)
     e2e_value = total_cells * e2e_steps / (e2e_ms * 1e-3)
@@ -382,6 +457,8 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
+        if batched is not None:
+            line["batched"] = batched
         line["cpu_baseline"] = cpu_baseline(w, budget_s=a.cpu_budget)
         print(json.dumps(line), flush=True)
     if dist is not None:

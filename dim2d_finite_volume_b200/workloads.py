@@ -1,0 +1,96 @@
+"""Seeded synthetic workloads of the benchmark configurations.
+
+Every domain is the DIM bubble set-up of ic.bubbles on [-0.5, 0.5]^2
+(saturated densities from the van der Waals Maxwell construction, tanh
+interface ~4 dx wide, uniform temperature T0), optionally carried by a
+uniform x-flow at a given Mach number of the liquid sound speed.  The time
+step is the smaller of the acoustic CFL step (CFL 0.1) and a viscous
+Fourier step, both from the initial state.
+
+"wall" domains use the reference's wall preset wall_S_reflection
+(library_config.py:102-115: contact-angle wall on S, mirrors elsewhere);
+the reference refuses wall_xy (library_config.py:93-99).
+"""
+import numpy as np
+
+from . import ic
+
+CV_R = 2.5
+RE = 5.0
+
+
+def liquid_sound_speed(T0, cv_r=CV_R):
+    rv, rl = ic.maxwell_densities(T0)
+    e = rl * (8.0 / 3.0 * cv_r * T0 - 3.0 * rl)
+    return float(ic.sound_speed(np.array(rl), np.array(0.0), np.array(0.0), np.array(e), cv_r))
+
+
+def stable_dt(q, dx, dy, cfl=0.1, fourier=0.2):
+    """min(acoustic CFL step, viscous Fourier step) over the interior."""
+    dt_a = ic.cfl_dt(q, dx, dy, cfl, CV_R)
+    rho_min = float(q[0, 2:-2, 2:-2].min())
+    return min(dt_a, fourier * RE * rho_min * min(dx, dy) ** 2)
+
+
+def fill_periodic_ghosts(q):
+    """Periodic ghost layers as field%ini leaves them
+    (periodic_xy/bc_operators_class.f:156-199)."""
+    ny, nx = q.shape[1], q.shape[2]
+    px, py = nx - 4, ny - 4
+    q[:, :, 0:2] = q[:, :, px:px + 2]
+    q[:, :, nx - 2:] = q[:, :, 2:4]
+    q[:, 0:2, :] = q[:, py:py + 2, :]
+    q[:, ny - 2:, :] = q[:, 2:4, :]
+    return q
+
+
+def domain(n, ny=None, T0=0.95, bubbles=((0.0, 0.0, 0.1),), mach=0.0, bc="periodic_xy"):
+    """One field: dict(nx, ny, x_map, y_map, nodes (4, ny, nx), dt, bc, T0, mach).
+    Mirror and wall fields still need their node boundary pass
+    (Field.apply_bc_on_nodes) after upload, as field%ini does."""
+    ny = n if ny is None else ny
+    nx, nyy, x_map, y_map = ic.grid(n, ny)
+    dx = x_map[1] - x_map[0]
+    dy = y_map[1] - y_map[0]
+    u0 = mach * liquid_sound_speed(T0) if mach else 0.0
+    q = ic.bubbles(x_map, y_map, T0, list(bubbles), li=4.0 * dx, velocity=(u0, 0.0))
+    if bc == "periodic_xy":
+        fill_periodic_ghosts(q)
+    q = np.ascontiguousarray(q)
+    return dict(nx=nx, ny=nyy, x_map=x_map, y_map=y_map, nodes=q, dt=stable_dt(q, dx, dy),
+                bc=bc, T0=T0, mach=mach)
+
+
+def plain_1024(seed, n=1024, bc="hedstrom_xy"):
+    """Plain FP64 at 1024^2: a bubble of seeded radius in [0.05, 0.15] at
+    T0 = 0.95 carried by a Mach 0.1 x-flow with open boundaries on all
+    sides (bc='periodic_xy': the same bubble at rest in a periodic box)."""
+    rng = np.random.default_rng(seed)
+    r = float(rng.uniform(0.05, 0.15))
+    d = domain(n, T0=0.95, bubbles=[(0.0, 0.0, r)], mach=0.1 if bc == "hedstrom_xy" else 0.0,
+               bc=bc)
+    d["radius"] = r
+    return d
+
+
+BATCH_KINDS = ("wall_S_reflection", "periodic_xy", "hedstrom_xy")
+
+
+def batched_domains(seed, count=64, sizes=tuple(range(128, 513, 64))):
+    """Batched FP64: `count` independent domains, n uniform in
+    {128, 192, ..., 512} (square), T0 in U[0.90, 0.99], bubble radius in
+    U[0.05, 0.2], boundary kind uniform over wall / periodic / open, flow
+    Mach in U[0, 0.1] for open domains (wall and periodic domains at rest)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(rng.choice(sizes))
+        T0 = float(rng.uniform(0.90, 0.99))
+        r = float(rng.uniform(0.05, 0.2))
+        mach = float(rng.uniform(0.0, 0.1))
+        bc = BATCH_KINDS[int(rng.integers(0, len(BATCH_KINDS)))]
+        d = domain(n, T0=T0, bubbles=[(0.0, 0.0, r)], mach=mach if bc == "hedstrom_xy" else 0.0,
+                   bc=bc)
+        d["radius"] = r
+        out.append(d)
+    return out
