@@ -168,6 +168,17 @@ int dim2d_ini_coordinates(int nx, int ny, double x_min, double x_max, double y_m
 int dim2d_create(const dim2d_params* p, int nx, int ny, const int bc_choice[8],
                  const int bc_type[8], const int bc_order[8], int precision,
                  dim2d_handle** out) {
+  return create_field(p, nx, ny, bc_choice, bc_type, bc_order, precision, nullptr, out);
+}
+
+}  // extern "C"
+
+// dim2d_create; with `pool` set, the buffers come from the device's
+// stream-ordered pool on that stream (no device-wide synchronisation on
+// allocation or release) and the field runs on `pool`
+int dim2d::create_field(const dim2d_params* p, int nx, int ny, const int bc_choice[8],
+                        const int bc_type[8], const int bc_order[8], int precision,
+                        cudaStream_t pool, dim2d_handle** out) {
   if (!p || !bc_choice || !bc_type || !bc_order || !out)
     return set_error(DIM2D_ERR_ARG, "create: null argument");
   *out = nullptr;
@@ -220,27 +231,32 @@ int dim2d_create(const dim2d_params* p, int nx, int ny, const int bc_choice[8],
     return cuda_error(e, "create: cudaGetDevice");
   }
   const size_t bytes = 4 * h->f.plane * sizeof(double);
+  h->pool = pool;
+  auto alloc = [&](double** b, size_t n) {
+    return pool ? cudaMallocAsync((void**)b, n, pool) : cudaMalloc(b, n);
+  };
   double** bufs[3] = {&h->A, &h->B, &h->C};
   for (double** b : bufs) {
-    e = cudaMalloc(b, bytes);
+    e = alloc(b, bytes);
     if (e != cudaSuccess) {
       cudaGetLastError();
       dim2d_destroy(h);
-      return set_error(DIM2D_ERR_NOMEM, "create: cudaMalloc of %zu bytes failed: %s", bytes,
+      return set_error(DIM2D_ERR_NOMEM, "create: allocation of %zu bytes failed: %s", bytes,
                        cudaGetErrorString(e));
     }
   }
-  e = cudaMalloc(&h->x_map, nx * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&h->y_map, ny * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&h->scalar, 4 * sizeof(double));
+  e = alloc(&h->x_map, nx * sizeof(double));
+  if (e == cudaSuccess) e = alloc(&h->y_map, ny * sizeof(double));
+  if (e == cudaSuccess) e = alloc(&h->scalar, 4 * sizeof(double));
   if (e == cudaSuccess) h->status = reinterpret_cast<unsigned int*>(h->scalar + 2);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !pool)
+    e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     cudaGetLastError();
     dim2d_destroy(h);
     return set_error(DIM2D_ERR_NOMEM, "create: allocation failed: %s", cudaGetErrorString(e));
   }
-  h->stream = h->own_stream;
+  h->stream = pool ? pool : h->own_stream;
   // keep never-written pitch padding and ghost cells defined
   for (double* b : {h->A, h->B, h->C}) cudaMemsetAsync(b, 0, bytes, h->stream);
   cudaMemsetAsync(h->scalar, 0, 4 * sizeof(double), h->stream);
@@ -248,19 +264,27 @@ int dim2d_create(const dim2d_params* p, int nx, int ny, const int bc_choice[8],
   return DIM2D_OK;
 }
 
+extern "C" {
+
 int dim2d_destroy(dim2d_handle* h) {
   if (!h) return DIM2D_OK;
   if (h->batch) dim2d_batch_remove(h->batch, h);
-  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->stream && !h->pool) cudaStreamSynchronize(h->stream);
   drop_graphs(h);
   for (cudaEvent_t ev : h->prof_ev) cudaEventDestroy(ev);
-  cudaFree(h->A);
-  cudaFree(h->B);
-  cudaFree(h->C);
-  cudaFree(h->x_map);
-  cudaFree(h->y_map);
-  cudaFree(h->scalar);
-  cudaFree(h->td);
+  // pooled buffers are released in stream order, after the queued work
+  auto release = [&](void* b) {
+    if (!b) return;
+    if (h->pool) cudaFreeAsync(b, h->pool);
+    else cudaFree(b);
+  };
+  release(h->A);
+  release(h->B);
+  release(h->C);
+  release(h->x_map);
+  release(h->y_map);
+  release(h->scalar);
+  release(h->td);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
   return DIM2D_OK;
@@ -452,7 +476,9 @@ int dim2d_time_dev(dim2d_handle* h, double* time_dev) {
   if (!h->uploaded) return set_error(DIM2D_ERR_NOT_READY, "time_dev: no state");
   const Field& f = h->f;
   cudaError_t e = cudaSuccess;
-  if (!h->td) e = cudaMalloc(&h->td, 4 * f.plane * sizeof(double));
+  if (!h->td)
+    e = h->pool ? cudaMallocAsync((void**)&h->td, 4 * f.plane * sizeof(double), h->pool)
+                : cudaMalloc(&h->td, 4 * f.plane * sizeof(double));
   if (e != cudaSuccess) return set_error(DIM2D_ERR_NOMEM, "time_dev: %s", cudaGetErrorString(e));
   // td_operators_class.f:150-154: every cell starts at debug_real
   e = launch_fill(h->td, 9.9692099683868690e+36, 4 * f.plane, h->stream);

@@ -40,6 +40,7 @@ struct dim2d_handle {
   bool uploaded = false;
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
+  cudaStream_t pool = nullptr;  // buffers from the stream-ordered pool on this stream
   long long launches = 0;
   // captured one-step graphs, one per buffer parity (which buffer holds
   // u^n); slot i is valid for graph_dt[i] and graph_A[i].  graph_dt = -1
@@ -72,6 +73,11 @@ namespace dim2d {
 int classify_mirrors(const int bc_choice[8], const int bc_type[8], int* south_wall,
                      int* corners_y);
 WallConst make_wall(const dim2d_params& p);
+// dim2d_create; pool != nullptr: stream-ordered allocations on `pool`,
+// which also becomes the field's stream
+int create_field(const dim2d_params* p, int nx, int ny, const int bc_choice[8],
+                 const int bc_type[8], const int bc_order[8], int precision, cudaStream_t pool,
+                 dim2d_handle** out);
 }  // namespace dim2d
 
 // dim2d_step.cu

@@ -94,3 +94,30 @@ def batched_domains(seed, count=64, sizes=tuple(range(128, 513, 64))):
         d["radius"] = r
         out.append(d)
     return out
+
+
+SERVED_KINDS = ("wall_S_reflection", "hedstrom_xy")
+
+
+def served_requests(seed, count, rate=50.0, n_range=(64, 1024), steps_range=(500, 20000)):
+    """Served stream: Poisson arrivals at `rate` per second; grid size n
+    (square) log-uniform in n_range, step count uniform in steps_range,
+    T0 in U[0.9, 0.99], wall or open boundaries, one bubble of radius in
+    U[0.05, 0.2] (open fields: Mach in U[0, 0.1]).  Each request carries
+    its arrival time (s) from the start of the stream."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    lo, hi = np.log(n_range[0]), np.log(n_range[1])
+    for i in range(count):
+        t += float(rng.exponential(1.0 / rate))
+        n = int(round(float(np.exp(rng.uniform(lo, hi)))))
+        steps = int(rng.integers(steps_range[0], steps_range[1] + 1))
+        T0 = float(rng.uniform(0.90, 0.99))
+        r = float(rng.uniform(0.05, 0.2))
+        bc = SERVED_KINDS[int(rng.integers(0, len(SERVED_KINDS)))]
+        mach = float(rng.uniform(0.0, 0.1)) if bc == "hedstrom_xy" else 0.0
+        d = domain(n, T0=T0, bubbles=[(0.0, 0.0, r)], mach=mach, bc=bc)
+        d.update(arrival=t, nsteps=steps, radius=r)
+        out.append(d)
+    return out

@@ -250,6 +250,39 @@ DIM2D_API long long dim2d_batch_cells(const dim2d_batch *b);
 DIM2D_API int dim2d_batch_set_stream(dim2d_batch *b, void *stream);
 DIM2D_API int dim2d_batch_destroy(dim2d_batch *b);
 
+/* ---- Serving loop: no counterpart in the reference.  Requests (a
+ * field's initial state, dt and step count) arrive at any time; the server
+ * keeps their fields resident in HBM, admits them in arrival order while
+ * their three device copies fit the memory budget, and advances all
+ * admitted fields together in batched chunks of up to chunk_steps steps
+ * (continuous batching: requests join and leave between chunks, the next
+ * chunk is queued while the host admits and retires).  Fields come from
+ * the device's stream-ordered pool; results land in pinned host memory.
+ * dim2d_server_poll drives the loop (wait != 0: block until the oldest
+ * queued chunk has finished); call it repeatedly.  FP64 requests. */
+typedef struct dim2d_server dim2d_server;
+/* mem_budget: bytes of device memory for fields (0 = free memory less a
+ * reserve; larger values are capped the same way) */
+DIM2D_API int dim2d_server_create(const dim2d_params *p, size_t mem_budget, int chunk_steps,
+                                  dim2d_server **out);
+/* copies the inputs; *id identifies the request */
+DIM2D_API int dim2d_server_submit(dim2d_server *s, int nx, int ny, const int bc_choice[8],
+                                  const int bc_type[8], const int bc_order[8], int precision,
+                                  const double *nodes, const double *x_map, const double *y_map,
+                                  double dt, long long nsteps, long long *id);
+/* *completed = requests completed by this call */
+DIM2D_API int dim2d_server_poll(dim2d_server *s, int wait, int *completed);
+/* DIM2D_ERR_NOT_READY until the request is complete; then copies its final
+ * nodes(nx,ny,4) and time, its latency (submit to completion, seconds),
+ * and forgets the request.  DIM2D_ERR_WALL_ROOT (nodes still copied) if a
+ * wall ghost-cell root failed during the solve. */
+DIM2D_API int dim2d_server_result(dim2d_server *s, long long id, double *nodes, double *t,
+                                  double *latency_s);
+/* out[8]: pending, active, copying, completed, cell-updates issued, bytes
+ * in use, budget bytes, most requests active at once */
+DIM2D_API int dim2d_server_stats(const dim2d_server *s, long long out[8]);
+DIM2D_API int dim2d_server_destroy(dim2d_server *s);
+
 /* field_abstract_class.f:286-315: dx = (x_max-x_min)/(nx-1-2*bc_size). */
 DIM2D_API int dim2d_ini_coordinates(int nx, int ny, double x_min, double x_max, double y_min,
                           double y_max, double *x_map, double *y_map);

@@ -1,0 +1,97 @@
+"""Serving loop (dim2d_server_*): requests arriving over time are admitted
+by free memory and advanced together in batched chunks; every result must
+be the same alone and in the mix.
+
+"Alone" is the request's field stepped by itself through dim2d_step; in
+the mix it shares batched launches with other requests, joining and
+leaving between chunks.  Bar (FP64): normwise <= 1e-12 over all cells of
+open fields and the interior of wall fields."""
+import numpy as np
+import pytest
+
+from tests.helpers import normwise_rel_err_all
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def F():
+    from dim2d_finite_volume_b200 import field
+    return field
+
+
+@pytest.fixture(scope="module")
+def S():
+    from dim2d_finite_volume_b200 import server
+    return server
+
+
+def _requests(count, seed, n_range=(36, 110)):
+    from dim2d_finite_volume_b200 import workloads
+    return workloads.served_requests(seed, count, rate=200.0, n_range=n_range,
+                                     steps_range=(20, 90))
+
+
+def _alone(F, r):
+    with F.Field(r["nx"], r["ny"], bc=r["bc"]) as fld:
+        fld.variant = 2
+        fld.ini(r["nodes"], r["x_map"], r["y_map"])
+        if r["bc"] != "hedstrom_xy":
+            fld.apply_bc_on_nodes()  # field%ini
+        fld.integrate(r["dt"], r["nsteps"])
+        return fld.download(), fld.time
+
+
+def _err(a, b, bc):
+    if bc == "hedstrom_xy":
+        return normwise_rel_err_all(a, b)
+    return normwise_rel_err_all(a[:, 2:-2, 2:-2], b[:, 2:-2, 2:-2])
+
+
+def test_results_same_alone_and_in_the_mix(F, S):
+    reqs = _requests(8, seed=21)
+    with S.Server(chunk_steps=16) as srv:
+        run = S.serve(srv, reqs, keep_results=True)
+    assert run["stats"]["completed"] == len(reqs)
+    assert run["stats"]["max_active"] >= 2  # requests overlapped on the device
+    for i, r in enumerate(reqs):
+        got, t = run["results"][i]
+        ref, t_ref = _alone(F, r)
+        assert np.isfinite(got).all()
+        assert np.all(_err(got, ref, r["bc"]) <= 1e-12), (i, r["nx"], r["bc"])
+        assert abs(t - t_ref) <= 1e-12 * t_ref
+        assert run["latencies"][i] > 0
+
+
+def test_admission_by_memory_budget(F, S):
+    reqs = _requests(6, seed=5, n_range=(60, 60))  # equal sizes
+    for r in reqs:
+        r["arrival"] = 0.0  # all at once
+    one = 3 * 4 * reqs[0]["ny"] * ((reqs[0]["nx"] + 15) // 16 * 16) * 8
+    with S.Server(mem_budget=2 * one + 65536, chunk_steps=10) as srv:
+        run = S.serve(srv, reqs, keep_results=True)
+        st = srv.stats()
+    assert st["completed"] == len(reqs)
+    assert st["max_active"] == 2  # the budget holds two fields
+    assert st["bytes_in_use"] == 0
+    for i, r in enumerate(reqs):
+        ref, _ = _alone(F, r)
+        assert np.all(_err(run["results"][i][0], ref, r["bc"]) <= 1e-12)
+
+
+def test_result_protocol(F, S):
+    reqs = _requests(1, seed=2)
+    r = reqs[0]
+    with S.Server(chunk_steps=8) as srv:
+        rid = srv.submit(r["nodes"], r["x_map"], r["y_map"], r["dt"], r["nsteps"], r["bc"])
+        assert srv.result(rid) is None  # not run yet
+        while srv.stats()["completed"] < 1:
+            srv.poll(wait=True)
+        nodes, t, lat = srv.result(rid)
+        assert lat > 0 and np.isfinite(nodes).all()
+        with pytest.raises(F.Dim2dError):
+            srv.result(rid)  # forgotten once read
+        with pytest.raises(F.Dim2dError):  # larger than the whole budget
+            big = np.zeros((4, 600, 600))
+            S.Server(mem_budget=1 << 20).submit(big, np.linspace(0, 1, 600),
+                                                np.linspace(0, 1, 600), 1e-6, 10)
