@@ -45,6 +45,7 @@ def _lib():
 
 
 NOT_READY = 7
+WALL_ROOT = 5
 STATS = ("pending", "active", "copying", "completed", "cell_updates", "bytes_in_use",
          "budget_bytes", "max_active")
 
@@ -81,7 +82,10 @@ class Server:
         return n.value
 
     def result(self, rid):
-        """(nodes, time, latency_s), or None while the request runs."""
+        """(nodes, time, latency_s, status), or None while the request runs.
+        status 0, or WALL_ROOT when a wall ghost-cell root failed during the
+        solve -- where the reference stops; nodes then hold the state the
+        solve ended with."""
         out = np.empty(self.shapes.get(rid, (4, 1, 1)))  # unknown ids: the library errors
         t = ctypes.c_double()
         lat = ctypes.c_double()
@@ -90,9 +94,10 @@ class Server:
                                         ctypes.byref(lat))
         if rc == NOT_READY:
             return None
-        _check(rc)
+        if rc != WALL_ROOT:
+            _check(rc)
         del self.shapes[rid]
-        return out, t.value, lat.value
+        return out, t.value, lat.value, rc
 
     def stats(self):
         v = (ctypes.c_longlong * 8)()
@@ -120,11 +125,13 @@ class Server:
 def serve(server, requests, keep_results=False):
     """Replay `requests` (dicts with arrival (s), nodes, x_map, y_map, dt,
     nsteps, bc) in real time: each is submitted at its arrival time, the
-    loop polls in between.  Returns dict(latencies, results (id -> nodes
-    if keep_results), wall_s, cell_updates, stats)."""
+    loop polls in between.  Returns dict(latencies, results (index ->
+    (nodes, time) if keep_results), failed (indices of requests whose wall
+    root failed), nonfinite (other requests whose final state is not
+    finite), wall_s, cell_updates, stats)."""
     order = sorted(range(len(requests)), key=lambda i: requests[i]["arrival"])
     ids = {}
-    out, lat = {}, {}
+    out, lat, failed, nonfinite = {}, {}, [], []
     t0 = time.perf_counter()
     nxt = 0
     while len(lat) < len(requests):
@@ -145,10 +152,15 @@ def serve(server, requests, keep_results=False):
                 continue
             i = ids.pop(rid)
             lat[i] = res[2]
+            if res[3]:
+                failed.append(i)
+            elif not np.isfinite(res[0]).all():
+                nonfinite.append(i)
             if keep_results:
                 out[i] = (res[0], res[1])
     wall = time.perf_counter() - t0
     cu = sum(r["nsteps"] * (r["nodes"].shape[1] - 4) * (r["nodes"].shape[2] - 4)
              for r in requests)
-    return dict(latencies=[lat[i] for i in range(len(requests))], results=out, wall_s=wall,
+    return dict(latencies=[lat[i] for i in range(len(requests))], results=out,
+                failed=sorted(failed), nonfinite=sorted(nonfinite), wall_s=wall,
                 cell_updates=cu, stats=server.stats())

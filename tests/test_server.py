@@ -53,6 +53,7 @@ def test_results_same_alone_and_in_the_mix(F, S):
     with S.Server(chunk_steps=16) as srv:
         run = S.serve(srv, reqs, keep_results=True)
     assert run["stats"]["completed"] == len(reqs)
+    assert run["failed"] == []
     assert run["stats"]["max_active"] >= 2  # requests overlapped on the device
     for i, r in enumerate(reqs):
         got, t = run["results"][i]
@@ -87,7 +88,8 @@ def test_result_protocol(F, S):
         assert srv.result(rid) is None  # not run yet
         while srv.stats()["completed"] < 1:
             srv.poll(wait=True)
-        nodes, t, lat = srv.result(rid)
+        nodes, t, lat, status = srv.result(rid)
+        assert status == 0
         assert lat > 0 and np.isfinite(nodes).all()
         with pytest.raises(F.Dim2dError):
             srv.result(rid)  # forgotten once read
