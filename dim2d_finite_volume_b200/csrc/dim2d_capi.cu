@@ -204,8 +204,6 @@ int dim2d::create_field(const dim2d_params* p, int nx, int ny, const int bc_choi
   if (south_wall && p->wall_heat_source_choice != 0 && !(p->wall_heat_source_variance > 0) &&
       p->wall_heat_source_choice == 2)
     return set_error(DIM2D_ERR_ARG, "create: gaussian heat source needs a positive variance");
-  if (precision != DIM2D_FP64)
-    return set_error(DIM2D_ERR_UNSUPPORTED, "create: mixed precision not provided by this build");
 
   dim2d_handle* h = new dim2d_handle();
   h->p = *p;

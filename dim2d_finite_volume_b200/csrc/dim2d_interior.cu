@@ -311,7 +311,7 @@ static cudaError_t set_smem_attr() {
 
 template <int MODE>
 static cudaError_t launch_mode(const StageArgs& a, cudaStream_t s) {
-  if (stage_uses_strip(a)) return launch_strip_stage(a, MODE, a.variant - 1, s);
+  if (stage_uses_strip(a)) return launch_strip_stage(a, MODE, strip_shape_of(a), s);
   cudaError_t e = set_smem_attr();
   if (e != cudaSuccess) return e;
   dim3 grid((a.f.nx - 2 * BC + TX - 1) / TX, (a.f.ny - 2 * BC + TY - 1) / TY);

@@ -49,6 +49,7 @@ struct StageArgs {
   int variant;                         // 0 = 32x8 CTA tiles, 1..5 = warp strips (shape-1)
   int open;                            // all sides open: strip launches also integrate the
                                        // ghost cells (their first CTAs)
+  int mixed;                           // DIM2D_MIXED: FP32 face pass (strip kernels)
   double t;                            // field time (constant over the stages)
   double xmap0, ymap0;                 // x_map(1), y_map(1): x_map(i) = xmap0 + (i-1) dx
   WallConst wall;
@@ -86,8 +87,14 @@ cudaError_t launch_strip_stage(const StageArgs& a, int mode, int shape, cudaStre
 inline bool strip_layout_ok(const StageArgs& a) {
   return a.f.pitch % 2 == 0 && reinterpret_cast<uintptr_t>(a.uin) % 16 == 0;
 }
-// 1 if the stage launch of `a` runs a strip kernel
-inline bool stage_uses_strip(const StageArgs& a) { return a.variant > 0 && strip_layout_ok(a); }
+// 1 if the stage launch of `a` runs a strip kernel (mixed precision always
+// does: the tile kernel has no FP32 face pass)
+inline bool stage_uses_strip(const StageArgs& a) {
+  return (a.variant > 0 || a.mixed) && strip_layout_ok(a);
+}
+// strip shape of a stage launch (variant 1..5; mixed fields on variant 0
+// use shape 1)
+inline int strip_shape_of(const StageArgs& a) { return a.variant > 0 ? a.variant - 1 : 1; }
 // 1 if the stage launch of `a` also covers the open-boundary ghost cells
 inline bool stage_fuses_open(const StageArgs& a) { return a.open && stage_uses_strip(a); }
 constexpr int NUM_VARIANTS = 6;

@@ -65,36 +65,51 @@ __host__ __device__ __forceinline__ double node_tcap(double r, double rxm, doubl
 }
 
 // Inputs of one face flux, in the face frame.  "a" is the node on the low
-// side of the face, "b" the node on the high side.
-struct FaceIn {
+// side of the face, "b" the node on the high side.  T = double for the FP64
+// path, float for the face pass of the mixed-precision path.
+template <typename T>
+struct FaceInT {
   // conservative values: rho, momentum along n, momentum along t, energy
-  double ra, rb, mna, mnb, mta, mtb, ea, eb;
+  T ra, rb, mna, mnb, mta, mtb, ea, eb;
   // primitives: velocity along n / t, pressure, Tcl, cp, Tcap
-  double una, unb, uta, utb, pa, pb, ta, tb, ca, cb, ka, kb;
+  T una, unb, uta, utb, pa, pb, ta, tb, ca, cb, ka, kb;
   // derivatives at the face
-  double drn, drt;  // d rho / dn, d rho / dt
-  double dunn;      // d u_n / dn
-  double dunt;      // d u_n / dt
-  double dutn;      // d u_t / dn
-  double dutt;      // d u_t / dt
-  double lap;       // d2 rho/dn2 + d2 rho/dt2
-  double dtn;       // d Tcl / dn
-  double dkn;       // d Tcap / dn
+  T drn, drt;  // d rho / dn, d rho / dt
+  T dunn;      // d u_n / dn
+  T dunt;      // d u_n / dt
+  T dutn;      // d u_t / dn
+  T dutt;      // d u_t / dt
+  T lap;       // d2 rho/dn2 + d2 rho/dt2
+  T dtn;       // d Tcl / dn
+  T dkn;       // d Tcap / dn
 };
+using FaceIn = FaceInT<double>;
+
+// Flux coefficients in FP32 for the mixed-precision face pass.
+struct FluxCoefF {
+  float ire, iwe, ipr, irepr, c15cv, two_mu, viscous_r;
+};
+__host__ __device__ inline FluxCoefF flux_coef_f32(const DimConst& k) {
+  return FluxCoefF{(float)k.ire,   (float)k.iwe,    (float)k.ipr,      (float)k.irepr,
+                   (float)k.c15cv, (float)k.two_mu, (float)k.viscous_r};
+}
 
 // Face flux of the 4 conservative variables; out = {mass, momentum_n,
 // momentum_t, energy}.  For an x-face n = x (dim2d_fluxes_module.f:103-117,
 // 193-222, 319-348, 445-477 and the parts they call); for a y-face n = y
 // (:145-159, 256-285, 382-411, 511-541), momentum_n is then momentum_y.
-__host__ __device__ __forceinline__ void face_flux(const FaceIn& f, const DimConst& k,
-                                                   double out[4]) {
-  const double avr = 0.5 * (f.ra + f.rb);
-  const double avmn = 0.5 * (f.mna + f.mnb);
-  const double avun = 0.5 * (f.una + f.unb);
-  const double avut = 0.5 * (f.uta + f.utb);
-  const double drn2 = f.drn * f.drn;
-  const double drt2 = f.drt * f.drt;
-  const double grad2 = drn2 + drt2;
+// DKN = false leaves out the energy term -(1/(Re Pr)) dTcap/dn of the
+// capillarity part (the mixed path adds it in FP64).
+template <typename T, typename K, bool DKN>
+__host__ __device__ __forceinline__ void face_flux_t(const FaceInT<T>& f, const K& k, T out[4]) {
+  const T h = T(0.5);
+  const T avr = h * (f.ra + f.rb);
+  const T avmn = h * (f.mna + f.mnb);
+  const T avun = h * (f.una + f.unb);
+  const T avut = h * (f.uta + f.utb);
+  const T drn2 = f.drn * f.drn;
+  const T drt2 = f.drt * f.drt;
+  const T grad2 = drn2 + drt2;
 
   // mass: f(momentum_n)
   out[0] = avmn;
@@ -103,30 +118,34 @@ __host__ __device__ __forceinline__ void face_flux(const FaceIn& f, const DimCon
   // mu du_t/dt; capillarity 1.5/cv f(cp) |grad rho|^2 + f(rho) lap rho
   // + 0.5 (drho_t^2 - drho_n^2)
   {
-    const double inv = 0.5 * (f.mna * f.una + f.mnb * f.unb) + 0.5 * (f.pa + f.pb);
-    const double vis = k.two_mu * f.dunn + k.viscous_r * f.dutt;
-    const double cap = k.c15cv * (0.5 * (f.ca + f.cb)) * grad2 + avr * f.lap +
-                       0.5 * (-drn2 + drt2);
+    const T inv = h * (f.mna * f.una + f.mnb * f.unb) + h * (f.pa + f.pb);
+    const T vis = k.two_mu * f.dunn + k.viscous_r * f.dutt;
+    const T cap = k.c15cv * (h * (f.ca + f.cb)) * grad2 + avr * f.lap + h * (-drn2 + drt2);
     out[1] = inv - k.ire * vis - k.iwe * cap;
   }
   // tangential momentum: inviscid f(m_t u_n); viscid du_n/dt + du_t/dn;
   // capillarity -drho_n drho_t
   {
-    const double inv = 0.5 * (f.mta * f.una + f.mtb * f.unb);
-    const double vis = f.dunt + f.dutn;
-    const double cap = -f.drn * f.drt;
+    const T inv = h * (f.mta * f.una + f.mtb * f.unb);
+    const T vis = f.dunt + f.dutn;
+    const T cap = -f.drn * f.drt;
     out[2] = inv - k.ire * vis - k.iwe * cap;
   }
   // energy
   {
-    const double inv = 0.5 * (f.ea * f.una + f.eb * f.unb) + 0.5 * (f.pa * f.una + f.pb * f.unb);
-    const double vis = avun * (k.two_mu * f.dunn + k.viscous_r * f.dutt) +
-                       avut * (f.dunt + f.dutn) + k.ipr * f.dtn;
-    const double cap = k.c15cv * (0.5 * (f.ca * f.una + f.cb * f.unb)) * grad2 + avmn * f.lap +
-                       0.5 * avun * (-drn2 + drt2) - f.drn * f.drt * avut -
-                       avr * f.drn * (f.dunn + f.dutt) - k.irepr * f.dkn;
+    const T inv = h * (f.ea * f.una + f.eb * f.unb) + h * (f.pa * f.una + f.pb * f.unb);
+    const T vis = avun * (k.two_mu * f.dunn + k.viscous_r * f.dutt) +
+                  avut * (f.dunt + f.dutn) + k.ipr * f.dtn;
+    T cap = k.c15cv * (h * (f.ca * f.una + f.cb * f.unb)) * grad2 + avmn * f.lap +
+            h * avun * (-drn2 + drt2) - f.drn * f.drt * avut - avr * f.drn * (f.dunn + f.dutt);
+    if (DKN) cap = cap - k.irepr * f.dkn;
     out[3] = inv - k.ire * vis - k.iwe * cap;
   }
+}
+
+__host__ __device__ __forceinline__ void face_flux(const FaceIn& f, const DimConst& k,
+                                                   double out[4]) {
+  face_flux_t<double, DimConst, true>(f, k, out);
 }
 
 // Flux through a wall face, in the face frame (out = {mass, momentum_n,

@@ -32,6 +32,7 @@ StageArgs make_stage_args(const dim2d_handle* h, const double* uin, double* uout
   a.wall_s = h->south_wall;
   a.variant = h->variant;
   a.open = h->open_all;
+  a.mixed = h->precision == DIM2D_MIXED;
   a.t = h->t;
   a.xmap0 = h->xmap0;
   a.ymap0 = h->ymap0;

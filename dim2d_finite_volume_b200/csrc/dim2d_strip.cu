@@ -201,12 +201,165 @@ __device__ __forceinline__ void y_face(const StageArgs& a, int sb, int st, int u
   G[3] = F[3];
 }
 
+// ---- mixed precision (DIM2D_MIXED) -----------------------------------
+// The node pass runs in FP64 -- the van der Waals inversion for u, v, P,
+// Tcl, 1/(3-rho) and Tcap -- and stores FP32 copies of rho, m_x, m_y, E
+// and of those quantities; the face pass (stencils and flux formulas)
+// reads the FP32 copies and runs in FP32.  Tcap stays FP64 and its normal
+// derivative, the third-derivative capillary term of the energy flux, is
+// added to the face's energy flux in FP64.  Divergence and RK update are
+// FP64 on the FP64 state.
+enum NodeF : int {
+  F_R = 0, F_MX, F_MY, F_E, F_U, F_V, F_P, F_TCL, F_CP, F_LAPH, F_GXH, F_GYH, NQF
+};
+constexpr int NM = 3;              // node rows (y-1 .. y+1)
+constexpr int F_ROW = NQF * PC;    // floats per node row
+constexpr int WARP_DOUBLES_MIX = NS * ST_ROW + NM * PC + (NM * F_ROW + 1) / 2;
+#define FQ(o, c, dc) reinterpret_cast<float*>(g_ring)[(o) + (c) * PC + (dc)]
+#define KQ(o, dc) g_ring[(o) + (dc)]
+
+// node quantities of column c0-1+lane of one row (as node_row) into the
+// float row fo and the FP64 Tcap row ko
+__device__ __forceinline__ void node_row_mix(int sm, int s0, int sp, int fo, int ko, double qrdx,
+                                             double qrdy, double hrdx2, double hrdy2,
+                                             const DimConst& k) {
+  const double r = ST(s0, 0, 1);
+  const double rw = ST(s0, 0, 0), re = ST(s0, 0, 2);
+  const double rs = ST(sm, 0, 1), rn = ST(sp, 0, 1);
+  const double mx = ST(s0, 1, 1), my = ST(s0, 2, 1), e = ST(s0, 3, 1);
+  const double tm = 3.0 - r;
+  const double inv = 1.0 / (r * tm);
+  const double ir = tm * inv;
+  const double cp = r * inv;
+  const double u = mx * ir, v = my * ir;
+  const double w = e - 0.5 * r * (u * u + v * v) + 3.0 * (r * r);
+  const double gxh = qrdx * (re - rw), gyh = qrdy * (rn - rs);
+  FQ(fo, F_R, 0) = (float)r;
+  FQ(fo, F_MX, 0) = (float)mx;
+  FQ(fo, F_MY, 0) = (float)my;
+  FQ(fo, F_E, 0) = (float)e;
+  FQ(fo, F_U, 0) = (float)u;
+  FQ(fo, F_V, 0) = (float)v;
+  FQ(fo, F_P, 0) = (float)(k.c3cv * cp * w - 3.0 * (r * r));
+  FQ(fo, F_TCL, 0) = (float)(ir * w);
+  FQ(fo, F_CP, 0) = (float)cp;
+  FQ(fo, F_LAPH, 0) = (float)(hrdx2 * ((rw - 2.0 * r) + re) + hrdy2 * ((rs - 2.0 * r) + rn));
+  FQ(fo, F_GXH, 0) = (float)gxh;
+  FQ(fo, F_GYH, 0) = (float)gyh;
+  KQ(ko, 0) = 2.0 * ir * (gxh * gxh + gyh * gyh);
+}
+
+// FP64 face inputs a wall face flux reads, from the FP32 face inputs
+__device__ __forceinline__ FaceIn wall_face_in(const FaceInT<float>& fi) {
+  FaceIn d{};
+  d.ra = fi.ra;
+  d.rb = fi.rb;
+  d.drn = fi.drn;
+  d.drt = fi.drt;
+  d.dutn = fi.dutn;
+  d.lap = fi.lap;
+  return d;
+}
+
+// x-face between columns x-1 and x of row y: fm/f0/fp = node rows y-1, y,
+// y+1, k0 = Tcap row y
+template <bool WALL>
+__device__ __forceinline__ void x_face_mix(const StageArgs& a, const FluxCoefF& kf, int fm, int f0,
+                                           int fp, int k0, int x, double F[4]) {
+  const DimConst& k = a.k;
+  FaceInT<float> fi;
+  fi.ra = FQ(f0, F_R, 0); fi.rb = FQ(f0, F_R, 1);
+  fi.mna = FQ(f0, F_MX, 0); fi.mnb = FQ(f0, F_MX, 1);
+  fi.mta = FQ(f0, F_MY, 0); fi.mtb = FQ(f0, F_MY, 1);
+  fi.ea = FQ(f0, F_E, 0); fi.eb = FQ(f0, F_E, 1);
+  fi.una = FQ(f0, F_U, 0); fi.unb = FQ(f0, F_U, 1);
+  fi.uta = FQ(f0, F_V, 0); fi.utb = FQ(f0, F_V, 1);
+  fi.pa = FQ(f0, F_P, 0); fi.pb = FQ(f0, F_P, 1);
+  fi.ta = FQ(f0, F_TCL, 0); fi.tb = FQ(f0, F_TCL, 1);
+  fi.ca = FQ(f0, F_CP, 0); fi.cb = FQ(f0, F_CP, 1);
+  fi.ka = fi.kb = 0.0f;
+  const float rdx = (float)a.rdx, q_rdy = 0.25f * (float)a.rdy;
+  fi.drn = rdx * (fi.rb - fi.ra);
+  fi.drt = FQ(f0, F_GYH, 0) + FQ(f0, F_GYH, 1);
+  fi.dunn = rdx * (fi.unb - fi.una);
+  fi.dunt = q_rdy * ((FQ(fp, F_U, 0) + FQ(fp, F_U, 1)) - (FQ(fm, F_U, 0) + FQ(fm, F_U, 1)));
+  fi.dutn = rdx * (fi.utb - fi.uta);
+  fi.dutt = q_rdy * ((FQ(fp, F_V, 0) + FQ(fp, F_V, 1)) - (FQ(fm, F_V, 0) + FQ(fm, F_V, 1)));
+  fi.lap = FQ(f0, F_LAPH, 0) + FQ(f0, F_LAPH, 1);
+  fi.dtn = rdx * (fi.tb - fi.ta);
+  fi.dkn = 0.0f;
+  const bool w_face = WALL && a.wall_w && x == BC;
+  const bool e_face = WALL && a.wall_e && x == a.f.nx - BC;
+  if (w_face || e_face) {
+    const int dc = w_face ? 1 : 0;
+    const double tl = k.c38cv * ((double)FQ(f0, F_TCL, dc) - k.iwe * KQ(k0, dc));
+    const double q = wall_heat_flux(a.wall, a.xmap0 + x * a.dx);
+    wall_face_flux(wall_face_in(fi), tl, a.dx, q, w_face ? q : -q, k, F);
+    return;
+  }
+  float Ff[4];
+  face_flux_t<float, FluxCoefF, false>(fi, kf, Ff);
+#pragma unroll
+  for (int v = 0; v < 4; v++) F[v] = (double)Ff[v];
+  // -(1/We) * (-(1/(Re Pr)) dTcap/dn), FP64
+  F[3] += k.iwe * k.irepr * (a.rdx * (KQ(k0, 1) - KQ(k0, 0)));
+}
+
+// y-face between rows yb and yb+1 of column x: fb/ft = node rows yb, yb+1,
+// kb/kt = their Tcap rows; output in conservative order
+template <bool WALL>
+__device__ __forceinline__ void y_face_mix(const StageArgs& a, const FluxCoefF& kf, int fb, int ft,
+                                           int kb, int kt, int x, int yb, double G[4]) {
+  const DimConst& k = a.k;
+  const int yt = yb + 1;
+  FaceInT<float> fi;
+  fi.ra = FQ(fb, F_R, 1); fi.rb = FQ(ft, F_R, 1);
+  fi.mna = FQ(fb, F_MY, 1); fi.mnb = FQ(ft, F_MY, 1);
+  fi.mta = FQ(fb, F_MX, 1); fi.mtb = FQ(ft, F_MX, 1);
+  fi.ea = FQ(fb, F_E, 1); fi.eb = FQ(ft, F_E, 1);
+  fi.una = FQ(fb, F_V, 1); fi.unb = FQ(ft, F_V, 1);
+  fi.uta = FQ(fb, F_U, 1); fi.utb = FQ(ft, F_U, 1);
+  fi.pa = FQ(fb, F_P, 1); fi.pb = FQ(ft, F_P, 1);
+  fi.ta = FQ(fb, F_TCL, 1); fi.tb = FQ(ft, F_TCL, 1);
+  fi.ca = FQ(fb, F_CP, 1); fi.cb = FQ(ft, F_CP, 1);
+  fi.ka = fi.kb = 0.0f;
+  const float rdy = (float)a.rdy, q_rdx = 0.25f * (float)a.rdx;
+  fi.drn = rdy * (fi.rb - fi.ra);
+  fi.drt = FQ(fb, F_GXH, 1) + FQ(ft, F_GXH, 1);
+  fi.dunn = rdy * (fi.unb - fi.una);
+  fi.dunt = q_rdx * ((FQ(fb, F_V, 2) + FQ(ft, F_V, 2)) - (FQ(fb, F_V, 0) + FQ(ft, F_V, 0)));
+  fi.dutn = rdy * (fi.utb - fi.uta);
+  fi.dutt = q_rdx * ((FQ(fb, F_U, 2) + FQ(ft, F_U, 2)) - (FQ(fb, F_U, 0) + FQ(ft, F_U, 0)));
+  fi.lap = FQ(fb, F_LAPH, 1) + FQ(ft, F_LAPH, 1);
+  fi.dtn = rdy * (fi.tb - fi.ta);
+  fi.dkn = 0.0f;
+  double F[4];
+  const bool s_face = WALL && a.wall_s && yt == BC;
+  const bool n_face = WALL && a.wall_n && yt == a.f.ny - BC;
+  if (s_face || n_face) {
+    const int fo = s_face ? ft : fb, ko = s_face ? kt : kb;
+    const double tl = k.c38cv * ((double)FQ(fo, F_TCL, 1) - k.iwe * KQ(ko, 1));
+    const double q = wall_heat_flux(a.wall, a.xmap0 + x * a.dx);
+    wall_face_flux(wall_face_in(fi), tl, a.dy, q, s_face ? q : -q, k, F);
+  } else {
+    float Ff[4];
+    face_flux_t<float, FluxCoefF, false>(fi, kf, Ff);
+#pragma unroll
+    for (int v = 0; v < 4; v++) F[v] = (double)Ff[v];
+    F[3] += k.iwe * k.irepr * (a.rdy * (KQ(kt, 1) - KQ(kb, 1)));
+  }
+  G[0] = F[0];
+  G[1] = F[2];
+  G[2] = F[1];
+  G[3] = F[3];
+}
+
 // boundary kinds of the strip kernel
 enum StripKind : int { K_PLAIN = 0, K_WALL = 1, K_OPEN = 2 };
 
 // grid: [ghost CTAs (K_OPEN only)] + sx * sy strip CTAs, x fastest
 // The work of strip CTA number b of one field (sx strips per row band).
-template <int H, int WPC, int MODE, bool WALL>
+template <int H, int WPC, int MODE, bool WALL, bool MIX>
 __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const Field f = a.f;
@@ -221,12 +374,17 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
   const double hrdx2 = 0.5 * a.rdx * a.rdx, hrdy2 = 0.5 * a.rdy * a.rdy;
 
   // ring row offsets (warp base + lane column)
-  const int wb = warp * WARP_DOUBLES + lane;
+  const int wb = warp * (MIX ? WARP_DOUBLES_MIX : WARP_DOUBLES) + lane;
   int s0 = wb, s1 = wb + ST_ROW, s2 = wb + 2 * ST_ROW;  // state rows
   const int ub = wb + NS * ST_ROW;
   int um = ub, u0 = ub + UV_ROW, u1 = ub + 2 * UV_ROW;  // velocity rows
   const int qbase = ub + NUV * UV_ROW;
   int q0 = qbase, q1 = qbase + Q_ROW;                   // node rows
+  // mixed precision: Tcap rows (doubles) and FP32 node rows (floats)
+  int km = ub, k0 = ub + PC, k1 = ub + 2 * PC;
+  const int fbase = 2 * (warp * WARP_DOUBLES_MIX + NS * ST_ROW + NM * PC) + lane;
+  int fm = fbase, f0 = fbase + F_ROW, f1 = fbase + 2 * F_ROW;
+  const FluxCoefF kf = flux_coef_f32(k);
 
   // prologue: node quantities of rows y0-1 (into um, q1) and y0 (into u0,
   // q0), bottom face of row y0; then state rows y0 .. y0+2 in s0 .. s2
@@ -238,15 +396,18 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
   load_row(a, c0, y0, lane, v);
   store_row(s0, lane, v);
   __syncwarp();
-  node_row(s1, s2, s0, um, q1, qrdx, qrdy, hrdx2, hrdy2, k);
+  if (MIX) node_row_mix(s1, s2, s0, fm, km, qrdx, qrdy, hrdx2, hrdy2, k);
+  else node_row(s1, s2, s0, um, q1, qrdx, qrdy, hrdx2, hrdy2, k);
   load_row(a, c0, y0 + 1, lane, v);
   __syncwarp();  // state row y0-2 is no longer read
   store_row(s1, lane, v);
   __syncwarp();
-  node_row(s2, s0, s1, u0, q0, qrdx, qrdy, hrdx2, hrdy2, k);
+  if (MIX) node_row_mix(s2, s0, s1, f0, k0, qrdx, qrdy, hrdx2, hrdy2, k);
+  else node_row(s2, s0, s1, u0, q0, qrdx, qrdy, hrdx2, hrdy2, k);
   __syncwarp();
   double Gb[4];
-  y_face<WALL>(a, s2, s0, um, u0, q1, q0, x, y0 - 1, Gb);
+  if (MIX) y_face_mix<WALL>(a, kf, fm, f0, km, k0, x, y0 - 1, Gb);
+  else y_face<WALL>(a, s2, s0, um, u0, q1, q0, x, y0 - 1, Gb);
   load_row(a, c0, y0 + 2, lane, v);
   __syncwarp();  // state row y0-1 is no longer read
   store_row(s2, lane, v);
@@ -274,11 +435,17 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
 #pragma unroll
       for (int v = 0; v < 4; v++) un[v] = __ldg(a.u0 + go + v * f.plane);
     }
-    node_row(s0, s1, s2, u1, q1, qrdx, qrdy, hrdx2, hrdy2, k);
+    if (MIX) node_row_mix(s0, s1, s2, f1, k1, qrdx, qrdy, hrdx2, hrdy2, k);
+    else node_row(s0, s1, s2, u1, q1, qrdx, qrdy, hrdx2, hrdy2, k);
     __syncwarp();
     double Fx[4], Gt[4];
-    x_face<WALL>(a, s0, um, u0, u1, q0, x, Fx);
-    y_face<WALL>(a, s0, s1, u0, u1, q0, q1, x, y, Gt);
+    if (MIX) {
+      x_face_mix<WALL>(a, kf, fm, f0, f1, k0, x, Fx);
+      y_face_mix<WALL>(a, kf, f0, f1, k0, k1, x, y, Gt);
+    } else {
+      x_face<WALL>(a, s0, um, u0, u1, q0, x, Fx);
+      y_face<WALL>(a, s0, s1, u0, u1, q0, q1, x, y, Gt);
+    }
     double Fr[4];
 #pragma unroll
     for (int v = 0; v < 4; v++) Fr[v] = __shfl_down_sync(0xffffffffu, Fx[v], 1);
@@ -333,10 +500,18 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
     const int tq = q0;
     q0 = q1;
     q1 = tq;
+    const int tf = fm;
+    fm = f0;
+    f0 = f1;
+    f1 = tf;
+    const int tk = km;
+    km = k0;
+    k0 = k1;
+    k1 = tk;
   }
 }
 
-template <int H, int WPC, int MINB, int MODE, int KIND>
+template <int H, int WPC, int MINB, int MODE, int KIND, bool MIX>
 __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost_ctas, int sx) {
   int b = blockIdx.x;
   if (KIND == K_OPEN) {
@@ -346,7 +521,7 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost
     }
     b -= ghost_ctas;
   }
-  strip_cta<H, WPC, MODE, KIND == K_WALL>(a, b, sx);
+  strip_cta<H, WPC, MODE, KIND == K_WALL, MIX>(a, b, sx);
 }
 
 // stage arguments of domain i of a batched launch
@@ -369,6 +544,7 @@ __device__ __forceinline__ StageArgs batch_stage_args(const BatchStageArgs& P, i
   a.wall_s = d.wall_s;
   a.variant = 0;
   a.open = 0;
+  a.mixed = 0;
   a.t = 0.0;
   a.xmap0 = d.xmap0;
   a.ymap0 = 0.0;
@@ -407,26 +583,32 @@ __global__ void __launch_bounds__(32 * WPC, MINB)
   }
   const int i = batch_domain<false>(P, b);
   const StageArgs a = batch_stage_args(P, i);
-  strip_cta<H, WPC, 1, KIND == K_WALL>(a, b - P.d[i].strip0, P.d[i].sx);
+  strip_cta<H, WPC, 1, KIND == K_WALL, false>(a, b - P.d[i].strip0, P.d[i].sx);
 }
 
 #undef ST
 #undef UV
 #undef NQ_
+#undef FQ
+#undef KQ
 
-template <int H, int WPC, int MINB, int MODE>
+template <int H, int WPC, int MINB, int MODE, bool MIX>
 const void* strip_fn(int kind) {
-  if (kind == K_WALL) return (const void*)k_strip<H, WPC, MINB, MODE, K_WALL>;
-  if (kind == K_OPEN) return (const void*)k_strip<H, WPC, MINB, MODE, K_OPEN>;
-  return (const void*)k_strip<H, WPC, MINB, MODE, K_PLAIN>;
+  if (kind == K_WALL) return (const void*)k_strip<H, WPC, MINB, MODE, K_WALL, MIX>;
+  if (kind == K_OPEN) return (const void*)k_strip<H, WPC, MINB, MODE, K_OPEN, MIX>;
+  return (const void*)k_strip<H, WPC, MINB, MODE, K_PLAIN, MIX>;
 }
 
 template <int H, int WPC, int MINB>
 cudaError_t launch_strip_shape(const StageArgs& a, int mode, cudaStream_t s) {
-  const size_t smem = (size_t)WPC * WARP_DOUBLES * sizeof(double);
+  const size_t smem =
+      (size_t)WPC * (a.mixed ? WARP_DOUBLES_MIX : WARP_DOUBLES) * sizeof(double);
   const bool wall = a.wall_w || a.wall_e || a.wall_s || a.wall_n;
   const int kind = a.open ? K_OPEN : (wall ? K_WALL : K_PLAIN);
-  const void* fn = mode == 0 ? strip_fn<H, WPC, MINB, 0>(kind) : strip_fn<H, WPC, MINB, 1>(kind);
+  const void* fn = a.mixed ? (mode == 0 ? strip_fn<H, WPC, MINB, 0, true>(kind)
+                                        : strip_fn<H, WPC, MINB, 1, true>(kind))
+                           : (mode == 0 ? strip_fn<H, WPC, MINB, 0, false>(kind)
+                                        : strip_fn<H, WPC, MINB, 1, false>(kind));
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int sx = (a.f.nx - 2 * BC + SW - 1) / SW;
