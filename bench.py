@@ -51,6 +51,11 @@ def parse():
                     help="stage-kernel variant 0..5, or 'auto' (the library's autotuner)")
     ap.add_argument("--batch-domains", type=int, default=64,
                     help="domains of the batched workload (0: skip it)")
+    ap.add_argument("--mixed-steps", type=int, default=10000,
+                    help="steps of the mixed-precision configuration (0: skip it)")
+    ap.add_argument("--mixed-n", type=int, default=2048)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="precision of the plain workload")
     ap.add_argument("--served", type=int, default=32,
                     help="requests of the served stream (0: skip it)")
     ap.add_argument("--cpu-budget", type=float, default=15.0,
@@ -318,6 +323,72 @@ def run_served(a):
     }
 
 
+def run_mixed(a, stream, F, torch):
+    """Mixed precision at 2048^2 (4 bubbles, T0 = 0.97, wall): the mixed
+    field and the FP64 field advanced side by side in blocks of 1000 steps;
+    after every block, the L2 and Linf errors of rho and rho E of the mixed
+    state relative to the FP64 state.  The FP64 path is the error reference
+    (it matches the oracle to 1e-10 in the parity tests)."""
+    from dim2d_finite_volume_b200 import workloads
+    d = workloads.mixed_2048(a.seed + 4, n=a.mixed_n)
+    nx, ny, dt = d["nx"], d["ny"], d["dt"]
+    cells = (nx - 4) * (ny - 4)
+    flds = {}
+    for prec in (F.MIXED, F.FP64):
+        fld = F.Field(nx, ny, bc="wall_S_reflection", precision=prec)
+        fld.set_stream(stream.cuda_stream)
+        fld.ini(d["nodes"], d["x_map"], d["y_map"])
+        fld.apply_bc_on_nodes()  # field%ini
+        fld.variant = 2
+        flds[prec] = fld
+    block = 1000 if a.mixed_steps >= 1000 else a.mixed_steps
+    ms = {F.MIXED: 0.0, F.FP64: 0.0}
+    errors = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for fld in flds.values():  # warm-up (graph capture), then restart from the IC
+        fld.integrate(dt, 3)
+        fld.ini(d["nodes"], d["x_map"], d["y_map"])
+        fld.apply_bc_on_nodes()
+    done = 0
+    status = "ok"
+    with torch.cuda.stream(stream):
+        while done < a.mixed_steps:
+            k = min(block, a.mixed_steps - done)
+            for prec, fld in flds.items():
+                e0.record(stream)
+                fld.integrate(dt, k)
+                e1.record(stream)
+                e1.synchronize()
+                ms[prec] += e0.elapsed_time(e1)
+            done += k
+            try:
+                qm = flds[F.MIXED].download()
+                qd = flds[F.FP64].download()
+            except F.Dim2dError as ex:  # wall root failure: where the reference stops
+                status = "stopped after %d steps: %s" % (done, ex)
+                break
+            row = {"step": done}
+            for name, v in (("rho", 0), ("rhoE", 3)):
+                a_, b_ = qm[v, 2:-2, 2:-2], qd[v, 2:-2, 2:-2]
+                row[name + "_linf"] = float(np.abs(a_ - b_).max() / np.abs(b_).max())
+                row[name + "_l2"] = float(np.sqrt(((a_ - b_) ** 2).sum() / (b_ ** 2).sum()))
+            errors.append(row)
+    for fld in flds.values():
+        fld.close()
+    vm = cells * done / (ms[F.MIXED] * 1e-3) if done else None
+    vd = cells * done / (ms[F.FP64] * 1e-3) if done else None
+    return {
+        "workload": "mixed precision %d^2: %d bubbles r in [0.05,0.1], T0=0.97, wall "
+                    "(wall_S_reflection), %d steps" % (a.mixed_n, len(d["bubbles"]), a.mixed_steps),
+        "value": vm, "unit": "cell-updates/s", "fp64_value": vd,
+        "vs_fp64": (vm / vd) if vm and vd else None, "steps_run": done, "status": status,
+        "errors_vs_fp64": errors, "error_bar": 1e-5,
+        "error_reference": "the FP64 path (matches the oracle to <= 1e-10 in the parity tests)",
+        "timing": "CUDA events around each 1000-step block of graph-replayed steps; downloads "
+                  "for the error check outside the timed blocks",
+    }
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -343,7 +414,7 @@ def main():
     cells = (nx - 4) * (ny - 4)
     dt = w["dt"]
     stream = torch.cuda.Stream()
-    fld = F.Field(nx, ny, bc=a.bc)
+    fld = F.Field(nx, ny, bc=a.bc, precision=F.MIXED if a.precision == "mixed" else F.FP64)
     fld.set_stream(stream.cuda_stream)
     fld.ini(w["nodes"], w["x_map"], w["y_map"])
     tune_ms = None
@@ -416,6 +487,7 @@ def main():
     if a.batch_domains > 0:
         bres = run_batched(a, stream, barrier, F, torch, flush)
     served = run_served(a) if a.served > 0 else None
+    mixed = run_mixed(a, stream, F, torch) if a.mixed_steps > 0 else None
 
     t = torch.tensor([step_ms, e2e_ms], dtype=torch.float64, device="cuda")
     if dist is not None:
@@ -470,7 +542,9 @@ def main():
             "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
             "n_gpus": world, "steps": a.steps, "warmup": max(3, a.warmup),
             "ms_per_step": step_ms / a.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "vs_baseline": None,
+            "dtype": "f64" if a.precision == "fp64" else "f32 face pass + f64 (mixed)",
+            "data": "synthetic",
             "config": {"workload": "plain FP64 DIM %d^2 (+2 ghosts) bubble, T0=0.95, "
                                    "Mach %.1f flow, RK3 step" % (a.n, 0.1 if a.bc == "hedstrom_xy"
                                                                  else 0.0), "bc": a.bc, "nx": nx, "ny": ny, "dt": dt,
@@ -495,6 +569,8 @@ def main():
         }
         if batched is not None:
             line["batched"] = batched
+        if mixed is not None:
+            line["mixed"] = mixed
         if served is not None:
             if dist is None:
                 line["served"] = served

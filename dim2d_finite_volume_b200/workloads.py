@@ -121,3 +121,19 @@ def served_requests(seed, count, rate=50.0, n_range=(64, 1024), steps_range=(500
         d.update(arrival=t, nsteps=steps, radius=r)
         out.append(d)
     return out
+
+
+def mixed_2048(seed, n=2048, count=4):
+    """Mixed-precision configuration: 2048^2, `count` bubbles of radius in
+    U[0.05, 0.1] at seeded non-overlapping centres (clear of the walls), in
+    liquid at T0 = 0.97, wall boundaries (wall_S_reflection), at rest."""
+    rng = np.random.default_rng(seed)
+    bub = []
+    while len(bub) < count:
+        r = float(rng.uniform(0.05, 0.1))
+        cx, cy = (float(v) for v in rng.uniform(-0.5 + r + 0.05, 0.5 - r - 0.05, 2))
+        if all((cx - x) ** 2 + (cy - y) ** 2 > (r + rr + 0.05) ** 2 for x, y, rr in bub):
+            bub.append((cx, cy, r))
+    d = domain(n, T0=0.97, bubbles=bub, mach=0.0, bc="wall_S_reflection")
+    d["bubbles"] = bub
+    return d
