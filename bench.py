@@ -44,7 +44,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--n", type=int, default=N_INTERIOR)
+    ap.add_argument("--size", dest="n", type=int, default=N_INTERIOR,
+                    help="interior cells per side of the plain workload")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--bc", default="hedstrom_xy", choices=["hedstrom_xy", "periodic_xy"])
     ap.add_argument("--variant", default="auto",
@@ -223,6 +224,22 @@ def run_reference(a, rank, world):
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def reduce_max(values, dist, device):
+    """Element-wise maximum over all ranks (every rank gets it): the
+    multi-rank timing rule -- the job takes as long as its slowest rank."""
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def whole_job_rate(units_per_rank, world, steps, max_ms):
+    """Units per second of the whole job: every rank processed
+    units_per_rank per step (weak scaling) in at most max_ms."""
+    return units_per_rank * world * steps / (max_ms * 1e-3)
 
 
 def run_batched(a, stream, barrier, F, torch, flush):
@@ -489,23 +506,18 @@ def main():
     served = run_served(a) if a.served > 0 else None
     mixed = run_mixed(a, stream, F, torch) if a.mixed_steps > 0 else None
 
-    t = torch.tensor([step_ms, e2e_ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    step_ms, e2e_ms = float(t[0]), float(t[1])
+    step_ms, e2e_ms = reduce_max([step_ms, e2e_ms], dist, "cuda")
     batched = None
     if bres is not None:
-        tb = torch.tensor([bres["batch_ms"], bres["plain_ms"]], dtype=torch.float64, device="cuda")
-        if dist is not None:
-            dist.all_reduce(tb, op=dist.ReduceOp.MAX)
-        bv = bres["cells_per_step"] * world * bres["steps"] / (float(tb[0]) * 1e-3)
-        pv = bres["cells_per_step"] * world * bres["plain_steps"] / (float(tb[1]) * 1e-3)
+        tb = reduce_max([bres["batch_ms"], bres["plain_ms"]], dist, "cuda")
+        bv = whole_job_rate(bres["cells_per_step"], world, bres["steps"], tb[0])
+        pv = whole_job_rate(bres["cells_per_step"], world, bres["plain_steps"], tb[1])
         peak_b, _ = measured_peaks()
         batched = {
             "workload": "batched FP64: %d seeded domains, n in {128,...,512}^2, T0 in "
                         "[0.90,0.99], r in [0.05,0.2], wall (wall_S_reflection) / periodic / "
                         "open mix, Mach in [0,0.1] on open domains" % bres["domains"],
-            "value": bv, "unit": "cell-updates/s", "ms_per_step": float(tb[0]) / bres["steps"],
+            "value": bv, "unit": "cell-updates/s", "ms_per_step": tb[0] / bres["steps"],
             "steps": bres["steps"], "cells_per_step": bres["cells_per_step"],
             "kinds": bres["kinds"], "shapes": bres["shapes"],
             "gpu_launches": bres["launches"],
@@ -518,9 +530,8 @@ def main():
                       "graph); plain: the same fields stepped one after another, each by its "
                       "own step graph; L2 flushed between steps",
         }
-    total_cells = cells * world
-    value = total_cells * a.steps / (step_ms * 1e-3)
-    e2e_value = total_cells * e2e_steps / (e2e_ms * 1e-3)
+    value = whole_job_rate(cells, world, a.steps, step_ms)
+    e2e_value = whole_job_rate(cells, world, e2e_steps, e2e_ms)
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
