@@ -308,8 +308,8 @@ def run_batched(a, stream, barrier, F, torch, flush):
 
 
 def run_served(a):
-    """Served stream: seeded Poisson arrivals (rate 50/s) of FP64 requests,
-    n log-uniform in [64, 1024], steps in [500, 20000], wall / open;
+    """Served stream: seeded Poisson arrivals (rate 50/s) of FP64 or mixed
+    requests, n log-uniform in [64, 1024], steps in [500, 20000], wall / open;
     replayed in real time through the serving loop."""
     from dim2d_finite_volume_b200 import server as Sm
     from dim2d_finite_volume_b200 import workloads
@@ -320,7 +320,8 @@ def run_served(a):
     return {
         "workload": "served stream: %d requests, Poisson arrivals at 50/s, n log-uniform in "
                     "[64,1024], steps uniform in [500,20000], T0 in [0.90,0.99], wall "
-                    "(wall_S_reflection) / open, FP64" % len(reqs),
+                    "(wall_S_reflection) / open, FP64 or mixed precision per request (%d mixed)"
+                    % (len(reqs), sum(r["precision"] for r in reqs)),
         "value": run["cell_updates"] / run["wall_s"], "unit": "cell-updates/s",
         "wall_s": run["wall_s"], "cell_updates": int(run["cell_updates"]),
         "latency_p50_s": float(np.percentile(lat, 50)),

@@ -11,7 +11,9 @@ import numpy as np
 
 from .field import Dim2dError, _check, library  # noqa: F401  (re-exported error type)
 
-GROUPS = ("periodic_xy", "hedstrom_xy", "wall_S_reflection", "reflection_xy")
+GROUPS = ("periodic_xy", "hedstrom_xy", "wall_S_reflection", "reflection_xy",
+          "periodic_xy/mixed", "hedstrom_xy/mixed", "wall_S_reflection/mixed",
+          "reflection_xy/mixed")
 NSHAPES = 5
 _bound = False
 
@@ -83,12 +85,13 @@ class Batch:
         _check(_lib().dim2d_batch_set_stream(self._h, ctypes.c_void_p(stream)))
 
     def autotune(self):
-        """Per group: the fastest strip shape; returns (shapes[4], times ms [4][5])."""
-        chosen = (ctypes.c_int * 4)()
-        times = np.zeros(4 * NSHAPES)
+        """Per group: the fastest strip shape; returns (shapes[8], times ms [8][5])."""
+        ng = len(GROUPS)
+        chosen = (ctypes.c_int * ng)()
+        times = np.zeros(ng * NSHAPES)
         _check(_lib().dim2d_batch_autotune(self._h, chosen,
                                            times.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
-        return list(chosen), times.reshape(4, NSHAPES)
+        return list(chosen), times.reshape(ng, NSHAPES)
 
     @property
     def size(self):

@@ -8,8 +8,9 @@
 //   G_OPEN      hedstrom_xy            ghost cells fused into the launch
 //   G_WALL      wall_S_reflection      strip kernel + node boundary pass
 //   G_MIRROR    reflection_xy          strip kernel + node boundary pass
+// and by precision (groups 4..7: the same kinds, DIM2D_MIXED fields).
 // One RK stage of a group is one batched launch over all its domains (plus
-// one batched node pass), so a step is at most 4 x 3 x 2 launches however
+// one batched node pass), so a step is at most 8 x 3 x 2 launches however
 // many domains there are.  The groups are independent: a captured step
 // graph holds one chain per group as parallel branches, so the kinds
 // overlap on the device.  Two graphs are kept, one per buffer parity
@@ -25,16 +26,21 @@
 using namespace dim2d;
 
 namespace {
-enum Group : int { G_PERIODIC = 0, G_OPEN, G_WALL, G_MIRROR, NGROUPS };
+enum Group : int { G_PERIODIC = 0, G_OPEN, G_WALL, G_MIRROR, NKINDS, NGROUPS = 2 * NKINDS };
 constexpr int NSHAPES = 5;  // strip shapes, as dim2d_set_variant 1..5
 
 int group_of(const dim2d_handle* h) {
-  if (h->periodic) return G_PERIODIC;
-  if (h->open_all) return G_OPEN;
-  return h->south_wall ? G_WALL : G_MIRROR;
+  const int mix = h->precision == DIM2D_MIXED ? NKINDS : 0;
+  if (h->periodic) return G_PERIODIC + mix;
+  if (h->open_all) return G_OPEN + mix;
+  return (h->south_wall ? G_WALL : G_MIRROR) + mix;
 }
-int kind_of(int g) { return g == G_OPEN ? BK_OPEN : (g == G_WALL ? BK_WALL : BK_PLAIN); }
-bool has_node_pass(int g) { return g == G_WALL || g == G_MIRROR; }
+int kind_of(int g) {
+  g %= NKINDS;
+  return g == G_OPEN ? BK_OPEN : (g == G_WALL ? BK_WALL : BK_PLAIN);
+}
+bool has_node_pass(int g) { return g % NKINDS == G_WALL || g % NKINDS == G_MIRROR; }
+bool is_mixed(int g) { return g >= NKINDS; }
 }  // namespace
 
 struct dim2d_batch {
@@ -46,7 +52,7 @@ struct dim2d_batch {
   std::vector<dim2d_handle*> m;
   std::vector<double> dt;
   dim2d_params p{};
-  int shape[NGROUPS] = {1, 1, 1, 1};
+  int shape[NGROUPS] = {1, 1, 1, 1, 1, 1, 1, 1};
   bool use_graphs = true;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   long long graph_launches[2] = {0, 0};
@@ -116,7 +122,7 @@ cudaError_t group_stage(dim2d_batch* b, int g, const std::vector<int>& idx, int 
       q.corners_y = h->corners_y;
       q.status = h->status;
     }
-    cudaError_t e = launch_strip_batch(P, kind_of(g), shape, s);
+    cudaError_t e = launch_strip_batch(P, kind_of(g), shape, is_mixed(g), s);
     b->launches++;
     if (e != cudaSuccess) return e;
     if (has_node_pass(g)) {
@@ -245,8 +251,6 @@ int dim2d_batch_add(dim2d_batch* b, dim2d_handle* h, double dt) {
   if (h->device != b->device)
     return set_error(DIM2D_ERR_ARG, "batch_add: field lives on device %d, batch on %d",
                      h->device, b->device);
-  if (h->precision != DIM2D_FP64)
-    return set_error(DIM2D_ERR_UNSUPPORTED, "batch_add: only FP64 fields are batched");
   if (!b->m.empty() && std::memcmp(&b->p, &h->p, sizeof(dim2d_params)) != 0)
     return set_error(DIM2D_ERR_UNSUPPORTED,
                      "batch_add: batch members must share the physical constants");
@@ -339,7 +343,7 @@ int dim2d_batch_sync(dim2d_batch* b) {
   return DIM2D_OK;
 }
 
-int dim2d_batch_autotune(dim2d_batch* b, int chosen[4], double* times_ms) {
+int dim2d_batch_autotune(dim2d_batch* b, int chosen[8], double* times_ms) {
   if (!b) return set_error(DIM2D_ERR_ARG, "batch_autotune: null batch");
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaError_t e = cudaEventCreate(&e0);

@@ -136,9 +136,10 @@ struct BatchStageArgs {
 // boundary kinds of a batched stage launch
 enum BatchKind : int { BK_PLAIN = 0, BK_WALL = 1, BK_OPEN = 2 };
 
-// one stage of every domain in P (shape as launch_strip_stage); fills the
-// CTA geometry fields of P.d
-cudaError_t launch_strip_batch(BatchStageArgs& P, int kind, int shape, cudaStream_t s);
+// one stage of every domain in P (shape as launch_strip_stage; mixed: the
+// DIM2D_MIXED face pass for all of them); fills the CTA geometry fields of P.d
+cudaError_t launch_strip_batch(BatchStageArgs& P, int kind, int shape, bool mixed,
+                               cudaStream_t s);
 
 struct NodeBcDomain {
   const double* utmp;

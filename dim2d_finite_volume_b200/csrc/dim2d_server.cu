@@ -284,8 +284,8 @@ int dim2d_server_submit(dim2d_server* s, int nx, int ny, const int bc_choice[8],
     return set_error(DIM2D_ERR_ARG, "server_submit: null argument");
   if (nx < 8 || ny < 8 || nsteps <= 0 || !(dt > 0) || !std::isfinite(dt))
     return set_error(DIM2D_ERR_ARG, "server_submit: bad size, dt or step count");
-  if (precision != DIM2D_FP64)
-    return set_error(DIM2D_ERR_UNSUPPORTED, "server_submit: the server runs FP64 requests");
+  if (precision != DIM2D_FP64 && precision != DIM2D_MIXED)
+    return set_error(DIM2D_ERR_ARG, "server_submit: unknown precision %d", precision);
   Request* r = new Request();
   r->bytes = request_bytes(nx, ny);
   if (r->bytes > s->budget) {

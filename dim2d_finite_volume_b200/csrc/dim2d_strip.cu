@@ -568,7 +568,7 @@ __device__ __forceinline__ int batch_domain(const BatchStageArgs& P, int b) {
 
 // One RK stage of every domain of a batch (one boundary kind): the ghost
 // CTAs of all domains first (open kind), then every domain's strip CTAs.
-template <int H, int WPC, int MINB, int KIND>
+template <int H, int WPC, int MINB, int KIND, bool MIX>
 __global__ void __launch_bounds__(32 * WPC, MINB)
     k_strip_batch(const __grid_constant__ BatchStageArgs P) {
   int b = blockIdx.x;
@@ -583,7 +583,7 @@ __global__ void __launch_bounds__(32 * WPC, MINB)
   }
   const int i = batch_domain<false>(P, b);
   const StageArgs a = batch_stage_args(P, i);
-  strip_cta<H, WPC, 1, KIND == K_WALL, false>(a, b - P.d[i].strip0, P.d[i].sx);
+  strip_cta<H, WPC, 1, KIND == K_WALL, MIX>(a, b - P.d[i].strip0, P.d[i].sx);
 }
 
 #undef ST
@@ -620,12 +620,18 @@ cudaError_t launch_strip_shape(const StageArgs& a, int mode, cudaStream_t s) {
   return cudaLaunchKernel(fn, dim3(blocks), dim3(32 * WPC), args, smem, s);
 }
 
+template <int H, int WPC, int MINB, bool MIX>
+const void* strip_batch_fn(int kind) {
+  return kind == BK_WALL   ? (const void*)k_strip_batch<H, WPC, MINB, K_WALL, MIX>
+         : kind == BK_OPEN ? (const void*)k_strip_batch<H, WPC, MINB, K_OPEN, MIX>
+                           : (const void*)k_strip_batch<H, WPC, MINB, K_PLAIN, MIX>;
+}
+
 template <int H, int WPC, int MINB>
-cudaError_t launch_strip_batch_shape(BatchStageArgs& P, int kind, cudaStream_t s) {
-  const size_t smem = (size_t)WPC * WARP_DOUBLES * sizeof(double);
-  const void* fn = kind == BK_WALL   ? (const void*)k_strip_batch<H, WPC, MINB, K_WALL>
-                   : kind == BK_OPEN ? (const void*)k_strip_batch<H, WPC, MINB, K_OPEN>
-                                     : (const void*)k_strip_batch<H, WPC, MINB, K_PLAIN>;
+cudaError_t launch_strip_batch_shape(BatchStageArgs& P, int kind, bool mixed, cudaStream_t s) {
+  const size_t smem = (size_t)WPC * (mixed ? WARP_DOUBLES_MIX : WARP_DOUBLES) * sizeof(double);
+  const void* fn = mixed ? strip_batch_fn<H, WPC, MINB, true>(kind)
+                         : strip_batch_fn<H, WPC, MINB, false>(kind);
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   long long ghost = 0, strips = 0;
@@ -646,15 +652,16 @@ cudaError_t launch_strip_batch_shape(BatchStageArgs& P, int kind, cudaStream_t s
 
 }  // namespace
 
-cudaError_t launch_strip_batch(BatchStageArgs& P, int kind, int shape, cudaStream_t s) {
+cudaError_t launch_strip_batch(BatchStageArgs& P, int kind, int shape, bool mixed,
+                               cudaStream_t s) {
   if (P.ndom <= 0) return cudaSuccess;
   if (P.ndom > BATCH_MAX) return cudaErrorInvalidValue;
   switch (shape) {
-    case 0: return launch_strip_batch_shape<8, 4, 4>(P, kind, s);
-    case 1: return launch_strip_batch_shape<16, 4, 4>(P, kind, s);
-    case 2: return launch_strip_batch_shape<16, 4, 5>(P, kind, s);
-    case 3: return launch_strip_batch_shape<16, 2, 8>(P, kind, s);
-    case 4: return launch_strip_batch_shape<16, 8, 2>(P, kind, s);
+    case 0: return launch_strip_batch_shape<8, 4, 4>(P, kind, mixed, s);
+    case 1: return launch_strip_batch_shape<16, 4, 4>(P, kind, mixed, s);
+    case 2: return launch_strip_batch_shape<16, 4, 5>(P, kind, mixed, s);
+    case 3: return launch_strip_batch_shape<16, 2, 8>(P, kind, mixed, s);
+    case 4: return launch_strip_batch_shape<16, 8, 2>(P, kind, mixed, s);
   }
   return cudaErrorInvalidValue;
 }

@@ -124,8 +124,8 @@ class Server:
 
 def serve(server, requests, keep_results=False):
     """Replay `requests` (dicts with arrival (s), nodes, x_map, y_map, dt,
-    nsteps, bc) in real time: each is submitted at its arrival time, the
-    loop polls in between.  Returns dict(latencies, results (index ->
+    nsteps, bc and optionally precision) in real time: each is submitted at
+    its arrival time, the loop polls in between.  Returns dict(latencies, results (index ->
     (nodes, time) if keep_results), failed (indices of requests whose wall
     root failed), nonfinite (other requests whose final state is not
     finite), wall_s, cell_updates, stats)."""
@@ -139,7 +139,7 @@ def serve(server, requests, keep_results=False):
         while nxt < len(order) and requests[order[nxt]]["arrival"] <= now:
             r = requests[order[nxt]]
             ids[server.submit(r["nodes"], r["x_map"], r["y_map"], r["dt"], r["nsteps"],
-                              r["bc"])] = order[nxt]
+                              r["bc"], r.get("precision", FP64))] = order[nxt]
             nxt += 1
         st = server.stats()
         busy = st["active"] + st["copying"] > 0

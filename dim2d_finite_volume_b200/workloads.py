@@ -99,13 +99,16 @@ def batched_domains(seed, count=64, sizes=tuple(range(128, 513, 64))):
 SERVED_KINDS = ("wall_S_reflection", "hedstrom_xy")
 
 
-def served_requests(seed, count, rate=50.0, n_range=(64, 1024), steps_range=(500, 20000)):
+def served_requests(seed, count, rate=50.0, n_range=(64, 1024), steps_range=(500, 20000),
+                    mixed_fraction=0.5):
     """Served stream: Poisson arrivals at `rate` per second; grid size n
     (square) log-uniform in n_range, step count uniform in steps_range,
     T0 in U[0.9, 0.99], wall or open boundaries, one bubble of radius in
-    U[0.05, 0.2] (open fields: Mach in U[0, 0.1]).  Each request carries
-    its arrival time (s) from the start of the stream."""
+    U[0.05, 0.2] (open fields: Mach in U[0, 0.1]), FP64 or mixed precision
+    (a `mixed_fraction` share, drawn from a separate seeded stream).  Each
+    request carries its arrival time (s) from the start of the stream."""
     rng = np.random.default_rng(seed)
+    rng_p = np.random.default_rng(seed + 7919)
     t = 0.0
     out = []
     lo, hi = np.log(n_range[0]), np.log(n_range[1])
@@ -118,7 +121,8 @@ def served_requests(seed, count, rate=50.0, n_range=(64, 1024), steps_range=(500
         bc = SERVED_KINDS[int(rng.integers(0, len(SERVED_KINDS)))]
         mach = float(rng.uniform(0.0, 0.1)) if bc == "hedstrom_xy" else 0.0
         d = domain(n, T0=T0, bubbles=[(0.0, 0.0, r)], mach=mach, bc=bc)
-        d.update(arrival=t, nsteps=steps, radius=r)
+        d.update(arrival=t, nsteps=steps, radius=r,
+                 precision=1 if rng_p.uniform() < mixed_fraction else 0)
         out.append(d)
     return out
 

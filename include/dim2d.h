@@ -227,13 +227,16 @@ DIM2D_API int dim2d_step_noalloc(const dim2d_params *p, int nx, int ny, const in
  * graph with one independent chain per kind (periodic_xy, hedstrom_xy,
  * wall_S_reflection, reflection_xy), so the kinds overlap on the device.
  * Members are fields created with dim2d_create and uploaded, on the
- * batch's device, FP64, sharing one dim2d_params; the batch borrows their
+ * batch's device, sharing one dim2d_params (FP64 and DIM2D_MIXED fields
+ * form separate groups); the batch borrows their
  * buffers and advances their state and time.  While a field is a member,
  * dim2d_step on it is refused; dim2d_download/dim2d_time_dev of a member
  * are ordered after the batch's queued steps.  dim2d_destroy of a member
  * removes it first. */
 typedef struct dim2d_batch dim2d_batch;
-#define DIM2D_BATCH_GROUPS 4 /* periodic, open, wall_S, reflection */
+/* groups: periodic, open, wall_S, reflection (FP64), then the same four for
+ * DIM2D_MIXED fields */
+#define DIM2D_BATCH_GROUPS 8
 DIM2D_API int dim2d_batch_create(dim2d_batch **out);
 /* add a field that advances by dt per step */
 DIM2D_API int dim2d_batch_add(dim2d_batch *b, dim2d_handle *h, double dt);
@@ -247,9 +250,9 @@ DIM2D_API int dim2d_batch_sync(dim2d_batch *b);
 DIM2D_API int dim2d_batch_set_shape(dim2d_batch *b, int group, int shape);
 DIM2D_API int dim2d_batch_set_graphs(dim2d_batch *b, int enable);
 /* Autotuner: times dry steps (dt = 0, stage buffers only) of each group
- * for the 5 strip shapes and keeps the fastest; chosen[4] receives the
- * shapes, times_ms (optional) 4 x 5 dry-step times (0 for empty groups). */
-DIM2D_API int dim2d_batch_autotune(dim2d_batch *b, int chosen[4], double *times_ms);
+ * for the 5 strip shapes and keeps the fastest; chosen[8] receives the
+ * shapes, times_ms (optional) 8 x 5 dry-step times (0 for empty groups). */
+DIM2D_API int dim2d_batch_autotune(dim2d_batch *b, int chosen[8], double *times_ms);
 DIM2D_API int dim2d_batch_size(const dim2d_batch *b);
 DIM2D_API long long dim2d_batch_launch_count(const dim2d_batch *b);
 /* interior cells of all members (cell-updates per batch step) */
@@ -266,7 +269,8 @@ DIM2D_API int dim2d_batch_destroy(dim2d_batch *b);
  * chunk is queued while the host admits and retires).  Fields come from
  * the device's stream-ordered pool; results land in pinned host memory.
  * dim2d_server_poll drives the loop (wait != 0: block until the oldest
- * queued chunk has finished); call it repeatedly.  FP64 requests. */
+ * queued chunk has finished); call it repeatedly.  Requests are FP64 or
+ * DIM2D_MIXED, each in its own precision. */
 typedef struct dim2d_server dim2d_server;
 /* mem_budget: bytes of device memory for fields (0 = free memory less a
  * reserve; larger values are capped the same way) */

@@ -205,3 +205,33 @@ def test_member_rules(oracle, F, B):
         odd.close()
         bt.remove(fld)
         fld.integrate(dt, 1)         # free again
+
+
+def test_fp64_and_mixed_members_in_one_batch(oracle, F, B):
+    """Mixed-precision members form their own groups; each member's result
+    equals the field alone: FP64 to 1e-12, mixed to 1e-6 (the FP32 face
+    pass of the batched kernel against the single-field kernel)."""
+    picks = [MIX[0], MIX[1], MIX[2], MIX[3]]
+    cases = [(p,) + _prepared(oracle, F, p, n, ny, s) for p, n, ny, s in picks]
+    fields, precs = [], []
+    with B.Batch() as bt:
+        for k, (p, nx, ny, x_map, y_map, q, dt) in enumerate(cases):
+            for prec in (F.FP64, F.MIXED):
+                fld = F.Field(nx, ny, bc=p, precision=prec)
+                fld.ini(q, x_map, y_map)
+                bt.add(fld, dt)
+                fields.append((k, fld))
+                precs.append(prec)
+        bt.step(6)
+        bt.sync()
+        for (k, fld), prec in zip(fields, precs):
+            p, nx, ny, x_map, y_map, q, dt = cases[k]
+            with F.Field(nx, ny, bc=p, precision=prec) as alone:
+                alone.variant = 2
+                alone.ini(q, x_map, y_map)
+                alone.integrate(dt, 6)
+                ref = alone.download()
+            bar = 1e-6 if prec == F.MIXED else 1e-12
+            assert np.all(_err(fld.download(), ref, p) <= bar), (p, prec)
+    for _, fld in fields:
+        fld.close()

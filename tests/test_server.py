@@ -33,7 +33,7 @@ def _requests(count, seed, n_range=(36, 110)):
 
 
 def _alone(F, r):
-    with F.Field(r["nx"], r["ny"], bc=r["bc"]) as fld:
+    with F.Field(r["nx"], r["ny"], bc=r["bc"], precision=r.get("precision", 0)) as fld:
         fld.variant = 2
         fld.ini(r["nodes"], r["x_map"], r["y_map"])
         if r["bc"] != "hedstrom_xy":
@@ -48,6 +48,12 @@ def _err(a, b, bc):
     return normwise_rel_err_all(a[:, 2:-2, 2:-2], b[:, 2:-2, 2:-2])
 
 
+def _bar(r):
+    """FP64 requests: 1e-12; mixed-precision requests (FP32 face pass in a
+    batched kernel vs the single-field kernel): 1e-6."""
+    return 1e-6 if r.get("precision", 0) else 1e-12
+
+
 def test_results_same_alone_and_in_the_mix(F, S):
     reqs = _requests(8, seed=21)
     with S.Server(chunk_steps=16) as srv:
@@ -59,7 +65,7 @@ def test_results_same_alone_and_in_the_mix(F, S):
         got, t = run["results"][i]
         ref, t_ref = _alone(F, r)
         assert np.isfinite(got).all()
-        assert np.all(_err(got, ref, r["bc"]) <= 1e-12), (i, r["nx"], r["bc"])
+        assert np.all(_err(got, ref, r["bc"]) <= _bar(r)), (i, r["nx"], r["bc"], r["precision"])
         assert abs(t - t_ref) <= 1e-12 * t_ref
         assert run["latencies"][i] > 0
 
@@ -77,7 +83,7 @@ def test_admission_by_memory_budget(F, S):
     assert st["bytes_in_use"] == 0
     for i, r in enumerate(reqs):
         ref, _ = _alone(F, r)
-        assert np.all(_err(run["results"][i][0], ref, r["bc"]) <= 1e-12)
+        assert np.all(_err(run["results"][i][0], ref, r["bc"]) <= _bar(r))
 
 
 def test_result_protocol(F, S):
