@@ -255,8 +255,14 @@ int dim2d_batch_add(dim2d_batch* b, dim2d_handle* h, double dt) {
     return set_error(DIM2D_ERR_UNSUPPORTED,
                      "batch_add: batch members must share the physical constants");
   if (h->f.pitch % 2 != 0) return set_error(DIM2D_ERR_UNSUPPORTED, "batch_add: odd pitch");
-  // the batch's work follows what was queued on the field's stream
-  cudaError_t e = cudaEventRecord(b->done, h->stream);
+  // the batch's work follows what was queued on the field's stream,
+  // including an asynchronous download of the field
+  cudaError_t e = cudaSuccess;
+  if (h->copy_pending) {
+    e = cudaStreamWaitEvent(h->stream, h->copy_done, 0);
+    h->copy_pending = false;
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(b->done, h->stream);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->done, 0);
   if (e != cudaSuccess) return cuda_error(e, "batch_add");
   if (b->m.empty()) b->p = h->p;

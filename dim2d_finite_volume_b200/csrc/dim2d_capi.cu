@@ -268,6 +268,12 @@ int dim2d_destroy(dim2d_handle* h) {
   if (!h) return DIM2D_OK;
   if (h->batch) dim2d_batch_remove(h->batch, h);
   if (h->stream && !h->pool) cudaStreamSynchronize(h->stream);
+  if (h->copy_stream) {
+    cudaStreamSynchronize(h->copy_stream);
+    cudaStreamDestroy(h->copy_stream);
+    cudaEventDestroy(h->copy_ready);
+    cudaEventDestroy(h->copy_done);
+  }
   drop_graphs(h);
   for (cudaEvent_t ev : h->prof_ev) cudaEventDestroy(ev);
   // pooled buffers are released in stream order, after the queued work
@@ -297,6 +303,7 @@ int dim2d_set_stream(dim2d_handle* h, void* stream) {
 int dim2d_sync(dim2d_handle* h) {
   if (!h) return set_error(DIM2D_ERR_ARG, "sync: null handle");
   cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess && h->copy_stream) e = cudaStreamSynchronize(h->copy_stream);
   if (e != cudaSuccess) return cuda_error(e, "sync");
   return DIM2D_OK;
 }
@@ -305,7 +312,9 @@ int dim2d_upload(dim2d_handle* h, const double* nodes, const double* x_map, cons
                  double t) {
   if (!h || !nodes || !x_map || !y_map) return set_error(DIM2D_ERR_ARG, "upload: null argument");
   const Field& f = h->f;
-  cudaError_t e = cudaMemcpy2DAsync(h->A, f.pitch * sizeof(double), nodes, f.nx * sizeof(double),
+  cudaError_t e = wait_copy_if(h, h->A);  // a pending asynchronous copy of A lands first
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(h->A, f.pitch * sizeof(double), nodes, f.nx * sizeof(double),
                                     f.nx * sizeof(double), 4 * (size_t)f.ny,
                                     cudaMemcpyHostToDevice, h->stream);
   if (e == cudaSuccess)
@@ -350,6 +359,62 @@ int dim2d_download(dim2d_handle* h, double* nodes, double* t) {
   return check_status(h);
 }
 
+int dim2d_download_async(dim2d_handle* h, double* nodes, double* t) {
+  if (!h || !nodes) return set_error(DIM2D_ERR_ARG, "download_async: null argument");
+  if (!h->uploaded) return set_error(DIM2D_ERR_NOT_READY, "download_async: no state");
+  if (h->batch) return set_error(DIM2D_ERR_ARG, "download_async: the field is in a batch");
+  cudaError_t e = cudaSuccess;
+  if (!h->copy_stream) {
+    e = cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->copy_ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->copy_done, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_error(e, "download_async");
+  }
+  // a previous copy of the other buffer may still be pending: order it first
+  if (h->copy_pending) e = cudaStreamWaitEvent(h->stream, h->copy_done, 0);
+  const Field& f = h->f;
+  if (e == cudaSuccess) e = cudaEventRecord(h->copy_ready, h->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(h->copy_stream, h->copy_ready, 0);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(nodes, f.nx * sizeof(double), h->A, f.pitch * sizeof(double),
+                          f.nx * sizeof(double), 4 * (size_t)f.ny, cudaMemcpyDeviceToHost,
+                          h->copy_stream);
+  if (e == cudaSuccess) e = cudaEventRecord(h->copy_done, h->copy_stream);
+  if (e != cudaSuccess) return cuda_error(e, "download_async");
+  h->copy_src = h->A;
+  h->copy_pending = true;
+  if (t) *t = h->t;
+  return DIM2D_OK;
+}
+
+int dim2d_copy_done(dim2d_handle* h) {
+  if (!h) return set_error(DIM2D_ERR_ARG, "copy_done: null handle");
+  if (!h->copy_done) return 1;
+  const cudaError_t e = cudaEventQuery(h->copy_done);
+  if (e == cudaSuccess) return 1;
+  if (e == cudaErrorNotReady) {
+    cudaGetLastError();
+    return 0;
+  }
+  return -cuda_error(e, "copy_done");
+}
+
+int dim2d_host_alloc(size_t bytes, void** p) {
+  if (!p) return set_error(DIM2D_ERR_ARG, "host_alloc: null argument");
+  *p = nullptr;
+  cudaError_t e = cudaMallocHost(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(DIM2D_ERR_NOMEM, "host_alloc: %zu bytes: %s", bytes, cudaGetErrorString(e));
+  }
+  return DIM2D_OK;
+}
+
+int dim2d_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+  return DIM2D_OK;
+}
+
 int dim2d_device_state(dim2d_handle* h, double** nodes, int* pitch) {
   if (!h) return set_error(DIM2D_ERR_ARG, "device_state: null handle");
   if (nodes) *nodes = h->A;
@@ -384,7 +449,7 @@ int dim2d_autotune(dim2d_handle* h, int* chosen, double* times_ms) {
       return DIM2D_OK;
     }
   }
-  cudaError_t e = cudaSuccess;
+  cudaError_t e = wait_copy_if(h, h->B);  // the dry steps write B and C
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -466,6 +531,8 @@ int dim2d_profile_read(dim2d_handle* h, double* ms, long long* launches) {
 int dim2d_apply_bc_on_nodes(dim2d_handle* h) {
   if (!h) return set_error(DIM2D_ERR_ARG, "apply_bc_on_nodes: null handle");
   if (!h->uploaded) return set_error(DIM2D_ERR_NOT_READY, "apply_bc_on_nodes: no state");
+  cudaError_t e = wait_copy_if(h, h->A);
+  if (e != cudaSuccess) return cuda_error(e, "apply_bc_on_nodes");
   return apply_bc_on_nodes(h, h->A, h->A);
 }
 

@@ -23,6 +23,11 @@ struct dim2d_handle {
   double xmap0 = 0, ymap0 = 0;     // x_map(1), y_map(1)
   int variant = 0;                 // stage-kernel variant (dim2d_set_variant)
   struct dim2d_batch* batch = nullptr;  // batch this field belongs to, if any
+  // dim2d_download_async: side stream, its events, and the buffer being copied
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t copy_ready = nullptr, copy_done = nullptr;
+  const double* copy_src = nullptr;
+  bool copy_pending = false;
   int bc_choice[8]{}, bc_type[8]{}, bc_order[8]{};
   int side_kind[8]{};
   dim2d::Field f{};
@@ -97,3 +102,6 @@ int check_status(dim2d_handle* h);
 void prof_begin(dim2d_handle* h);
 void prof_end(dim2d_handle* h);
 void drop_graphs(dim2d_handle* h);
+// before work on h->stream writes `target`: wait for a pending
+// dim2d_download_async copy whose source it is
+cudaError_t wait_copy_if(dim2d_handle* h, const double* target);

@@ -144,6 +144,12 @@ int rk3_step(dim2d_handle* h, double dt) {
   return DIM2D_OK;
 }
 
+cudaError_t wait_copy_if(dim2d_handle* h, const double* target) {
+  if (!h->copy_pending || target != h->copy_src) return cudaSuccess;
+  h->copy_pending = false;
+  return cudaStreamWaitEvent(h->stream, h->copy_done, 0);
+}
+
 void drop_graphs(dim2d_handle* h) {
   for (int i = 0; i < 2; i++) {
     if (h->graph_exec[i]) cudaGraphExecDestroy(h->graph_exec[i]);
@@ -198,6 +204,9 @@ int rk3_steps(dim2d_handle* h, double dt, int nsteps) {
     h->graph_dt = dt;
   }
   for (int s = 0; s < nsteps; s++) {
+    // stage 1 writes B: a pending asynchronous copy of B must land first
+    cudaError_t ew = wait_copy_if(h, h->B);
+    if (ew != cudaSuccess) return cuda_error(ew, "step");
     if (graphs) {
       int slot = -1;
       for (int i = 0; i < 2; i++)

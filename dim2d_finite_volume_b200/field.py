@@ -126,6 +126,10 @@ def library():
         "dim2d_time_dev": (ctypes.c_int, [H, _dp]),
         "dim2d_apply_bc_on_nodes": (ctypes.c_int, [H]),
         "dim2d_download": (ctypes.c_int, [H, _dp, ctypes.POINTER(ctypes.c_double)]),
+        "dim2d_download_async": (ctypes.c_int, [H, _dp, ctypes.POINTER(ctypes.c_double)]),
+        "dim2d_copy_done": (ctypes.c_int, [H]),
+        "dim2d_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]),
+        "dim2d_host_free": (ctypes.c_int, [ctypes.c_void_p]),
         "dim2d_cfl_dt": (ctypes.c_int, [H, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
         "dim2d_set_stream": (ctypes.c_int, [H, ctypes.c_void_p]),
         "dim2d_sync": (ctypes.c_int, [H]),
@@ -163,6 +167,19 @@ def default_params(**overrides):
     for k, v in overrides.items():
         setattr(p, k, v)
     return p
+
+
+def pinned_empty(shape):
+    """float64 array in pinned (page-locked) host memory, for
+    Field.download_async and fast uploads; freed with the array."""
+    import weakref
+    n = int(np.prod(shape))
+    p = ctypes.c_void_p()
+    _check(library().dim2d_host_alloc(max(8, n * 8), ctypes.byref(p)))
+    buf = (ctypes.c_double * max(1, n)).from_address(p.value)
+    arr = np.frombuffer(buf, dtype=np.float64, count=n).reshape(shape)
+    weakref.finalize(arr, library().dim2d_host_free, p)
+    return arr
 
 
 def _ptr(a):
@@ -220,6 +237,23 @@ class Field:
     # --- field_abstract_class.f:447-463 ----------------------------------
     def apply_bc_on_nodes(self):
         _check(library().dim2d_apply_bc_on_nodes(self._h))
+
+    def download_async(self, out):
+        """Queue a copy of the state into `out` (a pinned (4, ny, nx) array,
+        see pinned_empty) and return the state's time at once; the copy
+        overlaps the next integrate().  Read `out` after copy_done() or
+        sync()."""
+        if out.shape != (4, self.ny, self.nx):
+            raise ValueError("out must have shape (4, ny, nx)")
+        t = ctypes.c_double()
+        _check(library().dim2d_download_async(self._h, _ptr(out), ctypes.byref(t)))
+        return t.value
+
+    def copy_done(self):
+        rc = library().dim2d_copy_done(self._h)
+        if rc < 0:
+            _check(-rc)
+        return rc == 1
 
     def download(self, out=None):
         out = np.empty((4, self.ny, self.nx)) if out is None else out

@@ -159,6 +159,20 @@ DIM2D_API int dim2d_apply_bc_on_nodes(dim2d_handle *h);
 
 /* Copy the resident state (and time) back to the host; synchronises. */
 DIM2D_API int dim2d_download(dim2d_handle *h, double *nodes, double *t);
+/* No counterpart in the reference (its output is synchronous,
+ * io_operators_class.f): queue a copy of the resident state into host
+ * memory `nodes` (nodes(nx,ny,4) layout) on a side stream and return
+ * without waiting; *t receives the time of that state.  The copy overlaps
+ * the next dim2d_step; the step after it (the first to overwrite the
+ * copied buffer) waits for the copy, as do uploads and boundary passes.
+ * `nodes` must stay valid until the copy has landed: dim2d_copy_done
+ * returns 1 (0 while in flight), or after dim2d_sync.  For overlap, `nodes`
+ * must be pinned (dim2d_host_alloc).  Refused for batch members. */
+DIM2D_API int dim2d_download_async(dim2d_handle *h, double *nodes, double *t);
+DIM2D_API int dim2d_copy_done(dim2d_handle *h);
+/* pinned host memory for dim2d_download_async / dim2d_upload */
+DIM2D_API int dim2d_host_alloc(size_t bytes, void **p);
+DIM2D_API int dim2d_host_free(void *p);
 
 /* dt = cfl * min(dx,dy) / max over interior nodes of (c + |u|), speed of
  * sound from dim2d_prim_module.f:1179-1215, reduced on the device. */
@@ -166,7 +180,7 @@ DIM2D_API int dim2d_cfl_dt(dim2d_handle *h, double cfl, double *dt);
 
 /* Run on the given CUDA stream (cudaStream_t) instead of the handle's own. */
 DIM2D_API int dim2d_set_stream(dim2d_handle *h, void *stream);
-/* Wait for all work queued on the handle. */
+/* Wait for all work queued on the handle (asynchronous downloads included). */
 DIM2D_API int dim2d_sync(dim2d_handle *h);
 /* Device pointer of the resident nodes (layout: 4 planes of ny rows of
  * `pitch` doubles) -- for callers that keep fields in HBM. */
