@@ -40,7 +40,7 @@ constexpr int SW = 30;  // cells per strip
 constexpr int RC = 34;  // state columns in the ring: c0-2 .. c0+31
 constexpr int PC = 34;  // node-quantity columns: c0-1 .. c0+32 (the last two are
                         // padding read only by lane 31, whose faces are unused)
-constexpr int NS = 3;   // state rows (y .. y+2)
+constexpr int NS = 4;   // state rows (y .. y+2, and the row y+3 landing)
 constexpr int NUV = 3;  // velocity rows (y-1 .. y+1)
 constexpr int NQ = 2;   // rows of the other node quantities (y, y+1)
 // node quantities besides u, v; GXH/GYH = half the centred density
@@ -49,7 +49,8 @@ enum NodeQ : int { Q_P = 0, Q_TCL, Q_CP, Q_TCAP, Q_LAPH, Q_GXH, Q_GYH, NQV };
 constexpr int ST_ROW = 4 * RC;    // doubles per state row (4 variables)
 constexpr int UV_ROW = 2 * PC;    // doubles per velocity row
 constexpr int Q_ROW = NQV * PC;   // doubles per node-quantity row
-constexpr int WARP_DOUBLES = NS * ST_ROW + NUV * UV_ROW + NQ * Q_ROW;
+constexpr int UN_ROW = 4 * 32;    // u^n of one row of the strip's cells (4 variables)
+constexpr int WARP_DOUBLES = NS * ST_ROW + NUV * UV_ROW + NQ * Q_ROW + 2 * UN_ROW;
 
 extern __shared__ __align__(16) double g_ring[];
 
@@ -85,6 +86,48 @@ __device__ __forceinline__ void store_row(int o, int lane, const double2 v[4]) {
 #pragma unroll
     for (int q = 0; q < 4; q++) d[q * (RC / 2)] = v[q];
   }
+}
+
+// Asynchronous global -> shared copies (cp.async): the next state row and
+// the next row's u^n land in the ring while the warp computes, without
+// passing through registers.  Completion is per thread (commit / wait
+// groups); a __syncwarp after the wait makes the whole row visible.
+__device__ __forceinline__ void cp_async16(double* smem, const double* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+// wait until at most N of this thread's most recent groups are pending
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// state row `row` into the ring row at offset o (which includes the lane),
+// asynchronously: lane p < 17 copies the 16-byte pairs of columns
+// c0-2+2p, c0-1+2p of the 4 planes (addresses clamped as in load_row)
+__device__ __forceinline__ void async_row(const StageArgs& a, int c0, int row, int lane, int o) {
+  if (lane < 17) {
+    const int r = min(row, a.f.ny - 1);
+    const int xp = min(c0 - 2 + 2 * lane, a.f.pitch - 2);
+    const double* src = a.uin + (size_t)r * a.f.pitch + xp;
+    double* dst = g_ring + (o - lane) + 2 * lane;
+#pragma unroll
+    for (int q = 0; q < 4; q++) cp_async16(dst + q * RC, src + q * a.f.plane);
+  }
+}
+
+// u^n of row y at the lane's cell (clamped column) into the u^n ring row un
+__device__ __forceinline__ void async_un(const StageArgs& a, int x, int y, int un) {
+  const size_t go = (size_t)y * a.f.pitch + min(x, a.f.nx - 1 - BC);
+#pragma unroll
+  for (int v = 0; v < 4; v++) cp_async8(g_ring + un + v * 32, a.u0 + go + v * a.f.plane);
 }
 
 // node quantities of column c0-1+lane of one row: sm/s0/sp = state rows
@@ -214,7 +257,7 @@ enum NodeF : int {
 };
 constexpr int NM = 3;              // node rows (y-1 .. y+1)
 constexpr int F_ROW = NQF * PC;    // floats per node row
-constexpr int WARP_DOUBLES_MIX = NS * ST_ROW + NM * PC + (NM * F_ROW + 1) / 2;
+constexpr int WARP_DOUBLES_MIX = NS * ST_ROW + NM * PC + (NM * F_ROW + 1) / 2 + 2 * UN_ROW;
 #define FQ(o, c, dc) reinterpret_cast<float*>(g_ring)[(o) + (c) * PC + (dc)]
 #define KQ(o, dc) g_ring[(o) + (dc)]
 
@@ -372,46 +415,54 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
   const DimConst& k = a.k;
   const double qrdx = 0.25 * a.rdx, qrdy = 0.25 * a.rdy;
   const double hrdx2 = 0.5 * a.rdx * a.rdx, hrdy2 = 0.5 * a.rdy * a.rdy;
+  const bool need_un = MODE == 1 && a.stage != 1;
 
   // ring row offsets (warp base + lane column)
-  const int wb = warp * (MIX ? WARP_DOUBLES_MIX : WARP_DOUBLES) + lane;
-  int s0 = wb, s1 = wb + ST_ROW, s2 = wb + 2 * ST_ROW;  // state rows
+  const int wbase = warp * (MIX ? WARP_DOUBLES_MIX : WARP_DOUBLES);
+  const int wb = wbase + lane;
+  int s0 = wb, s1 = wb + ST_ROW, s2 = wb + 2 * ST_ROW, s3 = wb + 3 * ST_ROW;  // state rows
   const int ub = wb + NS * ST_ROW;
   int um = ub, u0 = ub + UV_ROW, u1 = ub + 2 * UV_ROW;  // velocity rows
   const int qbase = ub + NUV * UV_ROW;
   int q0 = qbase, q1 = qbase + Q_ROW;                   // node rows
   // mixed precision: Tcap rows (doubles) and FP32 node rows (floats)
   int km = ub, k0 = ub + PC, k1 = ub + 2 * PC;
-  const int fbase = 2 * (warp * WARP_DOUBLES_MIX + NS * ST_ROW + NM * PC) + lane;
+  const int fbase = 2 * (wbase + NS * ST_ROW + NM * PC) + lane;
   int fm = fbase, f0 = fbase + F_ROW, f1 = fbase + 2 * F_ROW;
   const FluxCoefF kf = flux_coef_f32(k);
+  // u^n rows (two, alternating), after the rest of the warp's region
+  const int unb = wbase + (MIX ? NS * ST_ROW + NM * PC + (NM * F_ROW + 1) / 2
+                               : NS * ST_ROW + NUV * UV_ROW + NQ * Q_ROW) + lane;
+  int un0 = unb, un1 = unb + UN_ROW;
 
-  // prologue: node quantities of rows y0-1 (into um, q1) and y0 (into u0,
-  // q0), bottom face of row y0; then state rows y0 .. y0+2 in s0 .. s2
+  // prologue: state rows y0-2, y0-1, y0, y0+1 (s3, s2, s0, s1); node
+  // quantities of rows y0-1 (um, q1) and y0 (u0, q0); bottom face of row
+  // y0; then row y0+2 (into s2) and u^n of row y0 on their way
   double2 v[4];
   load_row(a, c0, y0 - 2, lane, v);
-  store_row(s1, lane, v);
+  store_row(s3, lane, v);
   load_row(a, c0, y0 - 1, lane, v);
   store_row(s2, lane, v);
   load_row(a, c0, y0, lane, v);
   store_row(s0, lane, v);
-  __syncwarp();
-  if (MIX) node_row_mix(s1, s2, s0, fm, km, qrdx, qrdy, hrdx2, hrdy2, k);
-  else node_row(s1, s2, s0, um, q1, qrdx, qrdy, hrdx2, hrdy2, k);
   load_row(a, c0, y0 + 1, lane, v);
-  __syncwarp();  // state row y0-2 is no longer read
   store_row(s1, lane, v);
   __syncwarp();
-  if (MIX) node_row_mix(s2, s0, s1, f0, k0, qrdx, qrdy, hrdx2, hrdy2, k);
-  else node_row(s2, s0, s1, u0, q0, qrdx, qrdy, hrdx2, hrdy2, k);
+  if (MIX) {
+    node_row_mix(s3, s2, s0, fm, km, qrdx, qrdy, hrdx2, hrdy2, k);
+    node_row_mix(s2, s0, s1, f0, k0, qrdx, qrdy, hrdx2, hrdy2, k);
+  } else {
+    node_row(s3, s2, s0, um, q1, qrdx, qrdy, hrdx2, hrdy2, k);
+    node_row(s2, s0, s1, u0, q0, qrdx, qrdy, hrdx2, hrdy2, k);
+  }
   __syncwarp();
   double Gb[4];
   if (MIX) y_face_mix<WALL>(a, kf, fm, f0, km, k0, x, y0 - 1, Gb);
   else y_face<WALL>(a, s2, s0, um, u0, q1, q0, x, y0 - 1, Gb);
-  load_row(a, c0, y0 + 2, lane, v);
-  __syncwarp();  // state row y0-1 is no longer read
-  store_row(s2, lane, v);
-  __syncwarp();
+  __syncwarp();  // rows y0-2 and y0-1 are no longer read
+  async_row(a, c0, y0 + 2, lane, s2);
+  if (need_un) async_un(a, x, y0, un0);
+  cp_async_commit();
 
   const bool active = lane < SW && x <= f.nx - 1 - BC;
   int ix2 = -1;
@@ -421,20 +472,16 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
     else if (x >= f.nx - 2 * BC) ix2 = x - px;
   }
 
-  // s0/s1/s2 = state rows y, y+1, y+2; um/u0 = velocity rows y-1, y and u1
-  // the free row; q0 = node row y and q1 the free row
+  // s0/s1/s2 = state rows y, y+1, y+2 (row y+2 may still be landing), s3
+  // the free slot; un0 = u^n of row y (may be landing), un1 free; um/u0 =
+  // velocity rows y-1, y and u1 free; q0 = node row y and q1 free
 #pragma unroll 1
   for (int y = y0; y < y1; y++) {
-    double2 nxt[4];
-    load_row(a, c0, y + 3, lane, nxt);  // prefetch
-    // u^n of this row's cells (stages 2 and 3), issued before the node and
-    // face work so its latency is hidden; clamped column for unused lanes
-    const size_t go = (size_t)y * f.pitch + min(x, f.nx - 1 - BC);
-    double un[4] = {0.0, 0.0, 0.0, 0.0};
-    if (MODE == 1 && a.stage != 1) {
-#pragma unroll
-      for (int v = 0; v < 4; v++) un[v] = __ldg(a.u0 + go + v * f.plane);
-    }
+    async_row(a, c0, y + 3, lane, s3);  // next row: lands during this one
+    if (need_un) async_un(a, x, y + 1, un1);
+    cp_async_commit();
+    cp_async_wait<1>();  // all but the group just issued: rows y+2, u^n(y)
+    __syncwarp();
     if (MIX) node_row_mix(s0, s1, s2, f1, k1, qrdx, qrdy, hrdx2, hrdy2, k);
     else node_row(s0, s1, s2, u1, q1, qrdx, qrdy, hrdx2, hrdy2, k);
     __syncwarp();
@@ -451,6 +498,7 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
     for (int v = 0; v < 4; v++) Fr[v] = __shfl_down_sync(0xffffffffu, Fx[v], 1);
     {
       // every lane evaluates the update; only active lanes store
+      const size_t go = (size_t)y * f.pitch + min(x, f.nx - 1 - BC);
       const double uc[4] = {ST(s0, 0, 2), ST(s0, 1, 2), ST(s0, 2, 2), ST(s0, 3, 2)};
       double out[4];
 #pragma unroll
@@ -462,7 +510,7 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
         }
         if (MODE == 0) out[v] = L;
         else if (a.stage == 1) out[v] = uc[v] + a.dt * L;
-        else out[v] = a.b * un[v] + (1.0 - a.b) * (uc[v] + a.dt * L);
+        else out[v] = a.b * g_ring[un0 + v * 32] + (1.0 - a.b) * (uc[v] + a.dt * L);
       }
       if (active) {
 #pragma unroll
@@ -486,13 +534,15 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
     }
 #pragma unroll
     for (int v = 0; v < 4; v++) Gb[v] = Gt[v];
-    __syncwarp();  // state row y is no longer read
-    store_row(s0, lane, nxt);  // row y+3 takes the slot of row y
-    __syncwarp();
+    __syncwarp();  // row y and u^n(y) are no longer read
     const int t = s0;
     s0 = s1;
     s1 = s2;
-    s2 = t;
+    s2 = s3;
+    s3 = t;
+    const int tn = un0;
+    un0 = un1;
+    un1 = tn;
     const int tu = um;
     um = u0;
     u0 = u1;
@@ -509,6 +559,7 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
     k0 = k1;
     k1 = tk;
   }
+  cp_async_wait<0>();  // the copies of rows past the strip land before the warp exits
 }
 
 template <int H, int WPC, int MINB, int MODE, int KIND, bool MIX>
