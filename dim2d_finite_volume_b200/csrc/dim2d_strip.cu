@@ -61,33 +61,6 @@ extern __shared__ __align__(16) double g_ring[];
 #define UV(o, c, dc) g_ring[(o) + (c) * PC + (dc)]
 #define NQ_(o, c, dc) g_ring[(o) + (c) * PC + (dc)]
 
-// global loads of the state row `row` as 16-byte pairs: lane p < 17 reads
-// columns c0-2+2p and c0-1+2p of the 4 planes (lanes 17..31 repeat lane
-// 16).  Addresses are clamped to the field's rows and to its pitch, so no
-// load leaves the allocation; the clamped values land in ring columns that
-// only unused lanes read.  Needs an even pitch and 16-byte aligned planes
-// (strip_layout_ok).
-__device__ __forceinline__ void load_row(const StageArgs& a, int c0, int row, int lane,
-                                         double2 v[4]) {
-  const int r = min(row, a.f.ny - 1);
-  const int xp = min(c0 - 2 + 2 * min(lane, 16), a.f.pitch - 2);
-  const double2* p = reinterpret_cast<const double2*>(a.uin + (size_t)r * a.f.pitch + xp);
-  const size_t pl = a.f.plane / 2;
-  v[0] = __ldg(p);
-  v[1] = __ldg(p + pl);
-  v[2] = __ldg(p + 2 * pl);
-  v[3] = __ldg(p + 3 * pl);
-}
-
-// state row into the ring row at offset o (which includes the lane)
-__device__ __forceinline__ void store_row(int o, int lane, const double2 v[4]) {
-  if (lane < 17) {
-    double2* d = reinterpret_cast<double2*>(g_ring + (o - lane) + 2 * lane);
-#pragma unroll
-    for (int q = 0; q < 4; q++) d[q * (RC / 2)] = v[q];
-  }
-}
-
 // Asynchronous global -> shared copies (cp.async): the next state row and
 // the next row's u^n land in the ring while the warp computes, without
 // passing through registers.  Completion is per thread (commit / wait
@@ -111,7 +84,10 @@ __device__ __forceinline__ void cp_async_wait() {
 
 // state row `row` into the ring row at offset o (which includes the lane),
 // asynchronously: lane p < 17 copies the 16-byte pairs of columns
-// c0-2+2p, c0-1+2p of the 4 planes (addresses clamped as in load_row)
+// c0-2+2p, c0-1+2p of the 4 planes.  Addresses are clamped to the field's
+// rows and to its pitch, so no copy leaves the allocation; the clamped
+// values land in ring columns that only unused lanes read.  Needs an even
+// pitch and 16-byte aligned planes (strip_layout_ok).
 __device__ __forceinline__ void async_row(const StageArgs& a, int c0, int row, int lane, int o) {
   if (lane < 17) {
     const int r = min(row, a.f.ny - 1);
@@ -435,18 +411,16 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
                                : NS * ST_ROW + NUV * UV_ROW + NQ * Q_ROW) + lane;
   int un0 = unb, un1 = unb + UN_ROW;
 
-  // prologue: state rows y0-2, y0-1, y0, y0+1 (s3, s2, s0, s1); node
-  // quantities of rows y0-1 (um, q1) and y0 (u0, q0); bottom face of row
-  // y0; then row y0+2 (into s2) and u^n of row y0 on their way
-  double2 v[4];
-  load_row(a, c0, y0 - 2, lane, v);
-  store_row(s3, lane, v);
-  load_row(a, c0, y0 - 1, lane, v);
-  store_row(s2, lane, v);
-  load_row(a, c0, y0, lane, v);
-  store_row(s0, lane, v);
-  load_row(a, c0, y0 + 1, lane, v);
-  store_row(s1, lane, v);
+  // prologue: state rows y0-2, y0-1, y0, y0+1 (s3, s2, s0, s1), all four
+  // copies in flight together; node quantities of rows y0-1 (um, q1) and
+  // y0 (u0, q0); bottom face of row y0; then row y0+2 (into s2) and u^n of
+  // row y0 on their way
+  async_row(a, c0, y0 - 2, lane, s3);
+  async_row(a, c0, y0 - 1, lane, s2);
+  async_row(a, c0, y0, lane, s0);
+  async_row(a, c0, y0 + 1, lane, s1);
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncwarp();
   if (MIX) {
     node_row_mix(s3, s2, s0, fm, km, qrdx, qrdy, hrdx2, hrdy2, k);
