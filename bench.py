@@ -47,7 +47,10 @@ def parse():
     ap.add_argument("--size", dest="n", type=int, default=N_INTERIOR,
                     help="interior cells per side of the plain workload")
     ap.add_argument("--seed", type=int, default=1234)
-    ap.add_argument("--bc", default="hedstrom_xy", choices=["hedstrom_xy", "periodic_xy"])
+    ap.add_argument("--bc", default="hedstrom_xy",
+                    choices=["hedstrom_xy", "periodic_xy", "wall_S_reflection"])
+    ap.add_argument("--threads", type=int, default=0,
+                    help="host threads of the reference arm (0: all)")
     ap.add_argument("--variant", default="auto",
                     help="stage-kernel variant 0..5, or 'auto' (the library's autotuner)")
     ap.add_argument("--batch-domains", type=int, default=64,
@@ -152,12 +155,13 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def band_sample(w, rows):
-    """Rows [c - rows/2, c + rows/2) of the field around its centre line,
-    plus ghosts: the same per-cell work as the full field, bounded."""
+def band_sample(w, rows, bottom=False):
+    """Rows [c - rows/2, c + rows/2) of the field around its centre line
+    (bottom: the first rows, which hold the S wall), plus ghosts: the same
+    per-cell work as the full field, bounded."""
     ny = w["ny"]
     c = ny // 2
-    lo = max(0, c - rows // 2 - 2)
+    lo = 0 if bottom else max(0, c - rows // 2 - 2)
     hi = lo + rows + 4
     q = np.ascontiguousarray(w["nodes"][:, lo:hi, :])
     return q, np.ascontiguousarray(w["y_map"][lo:hi])
@@ -194,13 +198,18 @@ def run_reference(a, rank, world):
         return
     from oracle import oracle as O
     w = workload(a.n, a.seed, bc=a.bc)
-    nth = os.cpu_count() or 1
+    nth = a.threads or os.cpu_count() or 1
     O.set_threads(nth)
     nx = w["nx"]
-    q, y_map = band_sample(w, 32)
+    if w["ny"] <= 260:  # small fields are timed whole
+        q, y_map = np.ascontiguousarray(w["nodes"]), w["y_map"]
+    else:
+        q, y_map = band_sample(w, 32, bottom=a.bc == "wall_S_reflection")
     band = q.shape[1]
     cfg = oracle_cfg(O, a.bc, nx, band)
-    O.apply_bc_on_nodes(cfg, 0.0, w["x_map"], y_map, q.copy(), q)
+    if a.bc != "hedstrom_xy":  # field%ini: node boundary pass
+        O.lib().orc_clear_status()
+        O.apply_bc_on_nodes(cfg, 0.0, w["x_map"], y_map, q.copy(), q)
     cells = (nx - 4) * (band - 4)
     t = 0.0
     for _ in range(a.warmup):
@@ -215,11 +224,13 @@ def run_reference(a, rank, world):
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * el / a.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "impl": "reference",
-        "config": {"workload": "plain FP64 DIM %d^2 field, RK3 step, row-band sample" % a.n,
+        "config": {"workload": "plain FP64 DIM %d^2 field, RK3 step, %s" % (
+                       a.n, "whole field" if band == w["ny"] else "row-band sample"),
                    "sample_rows": band - 4, "bc": a.bc},
         "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": nth, "kind": "port",
-                         "sample": "each step: one RK3 step of a %dx%d band of the %d^2 field"
-                                   % (nx, band, a.n)},
+                         "sample": "each step: one RK3 step of %s of the %d^2 field"
+                                   % ("all %dx%d nodes" % (nx, band) if band == w["ny"]
+                                      else "a %dx%d band" % (nx, band), a.n)},
         "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -435,6 +446,8 @@ def main():
     fld = F.Field(nx, ny, bc=a.bc, precision=F.MIXED if a.precision == "mixed" else F.FP64)
     fld.set_stream(stream.cuda_stream)
     fld.ini(w["nodes"], w["x_map"], w["y_map"])
+    if a.bc not in ("periodic_xy", "hedstrom_xy"):
+        fld.apply_bc_on_nodes()  # field%ini
     tune_ms = None
     if a.variant == "auto":
         _, tune_ms = fld.autotune(measure=True)  # before the timed region
