@@ -255,6 +255,10 @@ int dim2d_batch_add(dim2d_batch* b, dim2d_handle* h, double dt) {
     return set_error(DIM2D_ERR_UNSUPPORTED,
                      "batch_add: batch members must share the physical constants");
   if (h->f.pitch % 2 != 0) return set_error(DIM2D_ERR_UNSUPPORTED, "batch_add: odd pitch");
+  if (h->open_mask && !h->open_all)
+    return set_error(DIM2D_ERR_UNSUPPORTED,
+                     "batch_add: wall_S_open / half_wall_S_open fields step on their own "
+                     "(no batched kernel for open sections beside a wall)");
   // the batch's work follows what was queued on the field's stream,
   // including an asynchronous download of the field
   cudaError_t e = cudaSuccess;

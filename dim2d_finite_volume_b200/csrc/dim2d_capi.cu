@@ -110,6 +110,37 @@ int classify_mirrors(const int bc_choice[8], const int bc_type[8], int* south_wa
   return 1;
 }
 
+int classify_open_wall(const int bc_choice[8], const int bc_type[8], const int bc_order[8],
+                       int* open_w) {
+  auto is = [&](int side, int choice, int type) {
+    return bc_choice[side] == choice && bc_type[side] == type;
+  };
+  auto open = [&](int side) { return is(side, DIM2D_HEDSTROM, DIM2D_BC_TIMEDEV); };
+  auto wall = [&](int side) { return is(side, DIM2D_WALL, DIM2D_BC_FLUX_AND_NODE); };
+  auto mirror = [&](int side) { return is(side, DIM2D_REFLECTION_X, DIM2D_BC_NODES); };
+  if (!open(DIM2D_SIDE_N) || !open(DIM2D_SIDE_E) || !open(DIM2D_SIDE_NE)) return 0;
+  if (!wall(DIM2D_SIDE_S) || !wall(DIM2D_SIDE_SE)) return 0;
+  int w;
+  if (open(DIM2D_SIDE_W) && open(DIM2D_SIDE_NW) && wall(DIM2D_SIDE_SW)) w = 1;
+  else if (mirror(DIM2D_SIDE_W) && mirror(DIM2D_SIDE_NW) && mirror(DIM2D_SIDE_SW)) w = 0;
+  else return 0;
+  if (!w) {
+    // half_wall_S_open: the S wall reads the W mirror ghosts, the SW corner
+    // mirrors the S wall ghosts (library_config.py:147 orders W, S, SE, SW)
+    int pos[9];
+    for (int i = 0; i < 9; i++) pos[i] = -1;
+    for (int k = 0; k < 8; k++)
+      if (bc_order[k] >= 1 && bc_order[k] <= 8) pos[bc_order[k]] = k;
+    if (pos[DIM2D_W_EDGE] < 0 || pos[DIM2D_S_EDGE] < 0 || pos[DIM2D_SW_CORNER] < 0 ||
+        pos[DIM2D_W_EDGE] > pos[DIM2D_S_EDGE] || pos[DIM2D_SW_CORNER] < pos[DIM2D_S_EDGE])
+      return -set_error(DIM2D_ERR_UNSUPPORTED,
+                       "create: half_wall_S_open needs the W edge before the S edge and the "
+                       "SW corner after it in bc_order");
+  }
+  *open_w = w;
+  return 1;
+}
+
 WallConst make_wall(const dim2d_params& p) {
   WallConst w{};
   w.cos_angle = std::cos(p.wall_micro_contact_angle * std::acos(-1.0) / 180.0);
@@ -197,10 +228,17 @@ int dim2d::create_field(const dim2d_params* p, int nx, int ny, const int bc_choi
   int south_wall = 0, corners_y = 0;
   const int mirrors = !periodic && !open && classify_mirrors(bc_choice, bc_type, &south_wall,
                                                              &corners_y);
-  if (!periodic && !open && !mirrors)
+  int open_w = 0;
+  int open_wall = 0;
+  if (!periodic && !open && !mirrors) {
+    open_wall = classify_open_wall(bc_choice, bc_type, bc_order, &open_w);
+    if (open_wall < 0) return -open_wall;
+    if (open_wall) south_wall = 1;
+  }
+  if (!periodic && !open && !mirrors && !open_wall)
     return set_error(DIM2D_ERR_UNSUPPORTED,
                      "create: boundary configuration not provided (periodic_xy, hedstrom_xy, "
-                     "reflection_xy and wall_S_reflection are)");
+                     "reflection_xy, wall_S_reflection, wall_S_open and half_wall_S_open are)");
   if (south_wall && p->wall_heat_source_choice != 0 && !(p->wall_heat_source_variance > 0) &&
       p->wall_heat_source_choice == 2)
     return set_error(DIM2D_ERR_ARG, "create: gaussian heat source needs a positive variance");
@@ -214,6 +252,12 @@ int dim2d::create_field(const dim2d_params* p, int nx, int ny, const int bc_choi
   h->mirrors = mirrors;
   h->south_wall = south_wall;
   h->corners_y = corners_y;
+  if (open) h->open_mask = OPEN_ALL;
+  if (open_wall) {
+    h->open_n = h->open_e = 1;
+    h->open_w = open_w;
+    h->open_mask = OPEN_N | OPEN_E | OPEN_NE | (open_w ? OPEN_W | OPEN_NW : 0);
+  }
   h->wall = make_wall(*p);
   std::memcpy(h->bc_choice, bc_choice, sizeof h->bc_choice);
   std::memcpy(h->bc_type, bc_type, sizeof h->bc_type);
@@ -438,7 +482,10 @@ int dim2d_get_variant(const dim2d_handle* h) { return h ? h->variant : -1; }
 int dim2d_autotune(dim2d_handle* h, int* chosen, double* times_ms) {
   if (!h) return set_error(DIM2D_ERR_ARG, "autotune: null handle");
   if (!h->uploaded) return set_error(DIM2D_ERR_NOT_READY, "autotune: no state");
-  const int cls = h->periodic ? 0 : (h->open_all ? 1 : (h->south_wall ? 2 : 3));
+  const int cls = h->periodic ? 0
+                  : h->open_all ? 1
+                  : h->open_mask ? 4 + h->open_w
+                  : h->south_wall ? 2 : 3;
   const long long key = ((long long)h->f.nx << 32) ^ ((long long)h->f.ny << 4) ^ cls;
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);

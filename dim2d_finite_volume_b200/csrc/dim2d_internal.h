@@ -16,8 +16,13 @@ struct dim2d_handle {
   int periodic = 0;
   int open_all = 0;  // hedstrom_xy: every section open, type bc_timedev
   int mirrors = 0;     // reflection_xy or wall_S_reflection (node pass kernel)
-  int south_wall = 0;  // wall_S_reflection
+  int south_wall = 0;  // wall on S: wall_S_reflection, wall_S_open, half_wall_S_open
   int corners_y = 0;   // corner sections are reflection_y
+  // open (Hedstrom) sections: dim2d::OPEN_* mask of the time-integrated ghost
+  // sections (all of them for hedstrom_xy) and the open sides of the mixed
+  // presets wall_S_open / half_wall_S_open
+  int open_mask = 0;
+  int open_w = 0, open_e = 0, open_n = 0;
   dim2d::WallConst wall{};
   unsigned int* status = nullptr;  // wall root status word (device)
   double xmap0 = 0, ymap0 = 0;     // x_map(1), y_map(1)
@@ -77,6 +82,12 @@ int all_open(const int bc_choice[8], const int bc_type[8]);
 namespace dim2d {
 int classify_mirrors(const int bc_choice[8], const int bc_type[8], int* south_wall,
                      int* corners_y);
+// wall_S_open or half_wall_S_open (library_config.py:118-150): returns 1
+// and sets *open_w (1 for wall_S_open, 0 for half_wall_S_open's mirror W);
+// returns minus an error code (set_error) for a section order the kernels
+// do not reproduce, 0 for any other configuration
+int classify_open_wall(const int bc_choice[8], const int bc_type[8], const int bc_order[8],
+                       int* open_w);
 WallConst make_wall(const dim2d_params& p);
 // dim2d_create; pool != nullptr: stream-ordered allocations on `pool`,
 // which also becomes the field's stream

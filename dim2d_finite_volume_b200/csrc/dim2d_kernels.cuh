@@ -35,6 +35,15 @@ __host__ __device__ __forceinline__ double wall_heat_flux(const WallConst& w, do
   return w.qmax * exp(-0.5 * (z * z));
 }
 
+// Ghost sections integrated with the open (Hedstrom, bc_timedev) operator:
+// bits of StageArgs::open.  hedstrom_xy sets all of them; wall_S_open sets
+// N, W, E, NW, NE; half_wall_S_open sets N, E, NE (library_config.py:118-150).
+enum OpenSection : int {
+  OPEN_S = 1, OPEN_N = 2, OPEN_W = 4, OPEN_E = 8,
+  OPEN_SW = 16, OPEN_SE = 32, OPEN_NW = 64, OPEN_NE = 128,
+  OPEN_ALL = 255
+};
+
 struct StageArgs {
   const double* __restrict__ uin;  // state the stencil reads
   const double* __restrict__ u0;   // u^n (stages 2 and 3)
@@ -47,8 +56,9 @@ struct StageArgs {
   int periodic;                    // write periodic ghost images of edge cells
   int wall_w, wall_e, wall_s, wall_n;  // wall flux override on that side
   int variant;                         // 0 = 32x8 CTA tiles, 1..5 = warp strips (shape-1)
-  int open;                            // all sides open: strip launches also integrate the
-                                       // ghost cells (their first CTAs)
+  int open;                            // OPEN_* mask of the time-integrated (Hedstrom)
+                                       // ghost sections; strip launches integrate those
+                                       // cells too (their first CTAs)
   int mixed;                           // DIM2D_MIXED: FP32 face pass (strip kernels)
   double t;                            // field time (constant over the stages)
   double xmap0, ymap0;                 // x_map(1), y_map(1): x_map(i) = xmap0 + (i-1) dx
@@ -56,16 +66,19 @@ struct StageArgs {
   DimConst k;
 };
 
-// Node boundary pass of a field whose sides are mirrors (reflection_x/_y)
-// or, on the south side, the wall operator.
+// Node boundary pass of a field whose sides are mirrors (reflection_x/_y),
+// open (nothing to do) or, on the south side, the wall operator.
 struct NodeBcArgs {
   const double* __restrict__ utmp;  // nodes_tmp = u^n (wall temperature guess)
   double* __restrict__ u;           // field whose ghosts are set
   Field f;
   double dx, dy, rdx, rdy;
   double t, xmap0, ymap0;
-  int south_wall;                   // 1: wall on S (wall_S_reflection), 0: mirror
+  int south_wall;                   // 1: wall on S, 0: mirror
   int corners_y;                    // corners are reflection_y (reflection_xy) vs _x
+  int open_w, open_e, open_n;       // side open (Hedstrom, integrated by the stage):
+                                    // no node work there; with a south wall its S corner
+                                    // is a wall corner (wall_S_open, half_wall_S_open)
   unsigned int* status;             // bit 0: root not bracketed, bits 1-3: Ridders
   WallConst wall;
   DimConst k;
@@ -100,7 +113,7 @@ inline bool stage_fuses_open(const StageArgs& a) { return a.open && stage_uses_s
 constexpr int NUM_VARIANTS = 6;
 // L(a.uin) of the interior cells into a.uout (stage fields ignored)
 cudaError_t launch_time_dev(const StageArgs& a, cudaStream_t s);
-// open (Hedstrom) ghost cells of a field open on all sides; mode 0 writes
+// open (Hedstrom) ghost cells of the sections in a.open; mode 0 writes
 // L(u) into a.uout, mode 1 the RK stage update
 cudaError_t launch_open_ghosts(const StageArgs& a, int mode, cudaStream_t s);
 cudaError_t launch_fill(double* p, double v, size_t n, cudaStream_t s);

@@ -102,6 +102,7 @@ extern "C" int dim2d_step_noalloc(const dim2d_params* p, int nx, int ny, const i
   h.precision = DIM2D_FP64;
   h.periodic = periodic;
   h.open_all = open;
+  h.open_mask = open ? OPEN_ALL : 0;
   for (int s = 0; s < 8; s++) {
     h.bc_choice[s] = bc_choice[s];
     h.bc_type[s] = bc_type[s];

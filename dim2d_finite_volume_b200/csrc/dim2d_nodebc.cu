@@ -1,15 +1,20 @@
 // dim2d_nodebc.cu -- node boundary pass for mirror sides and the south
 // wall on sm_100a.
 //
-// Configurations (the reference's presets, library_config.py:58-115):
+// Configurations (the reference's presets, library_config.py:58-150):
 //   reflection_xy      N/S reflection_y, E/W reflection_x, corners reflection_y
 //   wall_S_reflection  S wall, N reflection_y, E/W reflection_x, corners reflection_x
+//   wall_S_open        S, SW, SE wall; N, E, W, NE, NW open (no node work)
+//   half_wall_S_open   S, SE wall; W, SW, NW reflection_x; N, E, NE open
 // Mirrors: bc_operators_reflection_{x,y}_class.f:178-296 (prefactor -1 on
 // the normal momentum, reflection_xy_module.f:50-110).  Every mirror ghost
 // is a signed copy of an interior node, so all of them are computed
 // straight from the interior, in one launch, whatever the section order.
-// The corners of wall_S_reflection on the south side mirror the wall ghost
-// cells; the thread that solves a wall column writes them too.
+// The corners of wall_S_reflection (and the SW corner of half_wall_S_open)
+// mirror the wall ghost cells; the thread that solves a wall column writes
+// them too.  The wall corners next to an open side solve their ghost cells
+// like the wall edge, with one-sided tangential gradients in the outer
+// column.
 //
 // Wall ghost cell (wall_xy_equilibrium_module.f:948-1040, 1747-2461):
 // density of the first ghost row = root in [rho_vap(T), rho_liq(T)] of the
@@ -41,6 +46,11 @@ __host__ __device__ __forceinline__ int mirror_lo_hi(int i, int n) {
   return i < BC ? 2 * BC - 1 - i : 2 * n - 2 * BC - 1 - i;
 }
 
+// gradient type of a wall column along the wall (gradient_type of
+// compute_wall_*_ghost_cell, parameters_constant.f): centred, or one-sided
+// in the outer column of a wall corner
+enum WallGrad : int { WG_CENTRED = 0, WG_L0 = 1, WG_R0 = 2 };
+
 // wall root function context (wall_x_root_fct, :2016-2103)
 struct WallRoot {
   double md1;  // md_x(2): first interior density
@@ -50,6 +60,7 @@ struct WallRoot {
   double dxn, dyt;  // delta_x (normal), delta_y (tangential)
   double q;
   double cosang;
+  int gt;  // WallGrad of the tangential density gradient (get_dmd_dx, :2433-2461)
 };
 
 // dim2d_state_eq_module.f:56-227 (high-temperature fits)
@@ -61,7 +72,10 @@ __host__ __device__ double wall_root_f(const WallRoot& c, double x, const DimCon
   const double dmddx_half = (-c.md1 + x) / (c.dxn);
   const double md_av = 0.5 * (c.md1 + x);
   const double gx = (x - c.md2) / (2.0 * c.dxn);        // dmddx, interior type
-  const double gy = (c.my1 - c.my0) / (2.0 * c.dyt);    // dmddx, interior type
+  double gy;                                            // dmddx, :2433-2461
+  if (c.gt == WG_L0) gy = (c.my1 - c.md1) / c.dyt;
+  else if (c.gt == WG_R0) gy = (c.md1 - c.my0) / c.dyt;
+  else gy = (c.my1 - c.my0) / (2.0 * c.dyt);
   const double g2 = gx * gx + gy * gy;
   const double T1 = 3.0 / (8.0 * k.cv_r) *
                     (c.Ed / c.md1 - 0.5 * (c.vx * c.vx + c.vy * c.vy) -
@@ -160,27 +174,56 @@ __host__ __device__ __forceinline__ double ld(const double* p, const Field& f, i
 
 }  // namespace
 
-__host__ __device__ int node_bc_count(const NodeBcArgs& a) {
+// Work items of the node pass, in order: W mirror cells, E mirror cells,
+// N mirror cells (each only where that side is a mirror), S cells (wall
+// columns or mirror cells), then the corner cells that have node work.
+// Wall columns span the interior columns plus, on an open side, its two
+// ghost columns (the wall corner sections of wall_S_open /
+// half_wall_S_open, bc_operators_wall_xy_class.f:340-360).  Corner work:
+// mirror corners of reflection_xy (4) and wall_S_reflection (N only: the S
+// ones are written with their wall columns), and the reflection_x NW
+// corner of half_wall_S_open, which mirrors the open N ghost rows.
+struct NodeLayout {
+  int n_w, n_e, n_n, n_s;
+  int x0, x1;        // wall columns [x0, x1)
+  int corners;       // bit c: corner c (0 SW, 1 SE, 2 NW, 3 NE) has node work
+};
+
+__host__ __device__ __forceinline__ NodeLayout node_layout(const NodeBcArgs& a) {
   const int ex = a.f.nx - 2 * BC, ey = a.f.ny - 2 * BC;
-  const int n_we = 2 * BC * ey, n_n = BC * ex, n_s = a.south_wall ? ex : BC * ex;
-  const int n_c = (a.south_wall ? 2 : 4) * BC * BC;
-  return n_we + n_n + n_s + n_c;
+  NodeLayout L;
+  L.n_w = a.open_w ? 0 : BC * ey;
+  L.n_e = a.open_e ? 0 : BC * ey;
+  L.n_n = a.open_n ? 0 : BC * ex;
+  L.x0 = a.open_w ? 0 : BC;
+  L.x1 = a.open_e ? a.f.nx : a.f.nx - BC;
+  L.n_s = a.south_wall ? L.x1 - L.x0 : BC * ex;
+  L.corners = 0;
+  if (!a.south_wall) L.corners |= 3;
+  if (!a.open_w) L.corners |= 4;
+  if (!a.open_e) L.corners |= 8;
+  return L;
 }
 
-// Ghost work item m: W/E mirror cells, N mirror cells, S cells (wall
-// columns or mirror cells), then corner cells.
+__host__ __device__ int node_bc_count(const NodeBcArgs& a) {
+  const NodeLayout L = node_layout(a);
+  const int nc = (L.corners & 1) + (L.corners >> 1 & 1) + (L.corners >> 2 & 1) + (L.corners >> 3 & 1);
+  return L.n_w + L.n_e + L.n_n + L.n_s + nc * BC * BC;
+}
+
+// Ghost work item m (NodeLayout order)
 __host__ __device__ void node_bc_cell(const NodeBcArgs& a, int m) {
   const Field f = a.f;
   const int nx = f.nx, ny = f.ny;
   const int ex = nx - 2 * BC, ey = ny - 2 * BC;
-  const int n_we = 2 * BC * ey, n_n = BC * ex, n_s = a.south_wall ? ex : BC * ex;
+  const NodeLayout L = node_layout(a);
   if (m < 0 || m >= node_bc_count(a)) return;
   const double pre_x[4] = {1.0, -1.0, 1.0, 1.0};
   const double pre_y[4] = {1.0, 1.0, -1.0, 1.0};
   double* u = a.u;
-  if (m < n_we) {  // reflection_x, bc_operators_reflection_x_class.f:212-234
-    const bool east = m >= BC * ey;
-    const int r = east ? m - BC * ey : m;
+  if (m < L.n_w + L.n_e) {  // reflection_x, bc_operators_reflection_x_class.f:212-234
+    const bool east = m >= L.n_w;
+    const int r = east ? m - L.n_w : m;
     const int y = BC + r % ey;
     const int col = r / ey;
     const int x = east ? nx - BC + col : col;
@@ -189,8 +232,8 @@ __host__ __device__ void node_bc_cell(const NodeBcArgs& a, int m) {
       NBC_ST(&u[(size_t)v * f.plane + (size_t)y * f.pitch + x], pre_x[v] * ld(u, f, v, sx, y));
     return;
   }
-  m -= n_we;
-  if (m < n_n) {  // reflection_y, bc_operators_reflection_y_class.f:211-221
+  m -= L.n_w + L.n_e;
+  if (m < L.n_n) {  // reflection_y, bc_operators_reflection_y_class.f:211-221
     const int x = BC + m % ex;
     const int y = ny - BC + m / ex;
     const int sy = mirror_lo_hi(y, ny);
@@ -198,8 +241,8 @@ __host__ __device__ void node_bc_cell(const NodeBcArgs& a, int m) {
       NBC_ST(&u[(size_t)v * f.plane + (size_t)y * f.pitch + x], pre_y[v] * ld(u, f, v, x, sy));
     return;
   }
-  m -= n_n;
-  if (m < n_s) {
+  m -= L.n_n;
+  if (m < L.n_s) {
     if (!a.south_wall) {  // reflection_y, :223-233
       const int x = BC + m % ex;
       const int y = m / ex;
@@ -210,17 +253,24 @@ __host__ __device__ void node_bc_cell(const NodeBcArgs& a, int m) {
     }
     // wall ghost column x: ghost rows 1 (first) and 0 (second),
     // interior rows 2 (first) and 3 (second)
-    const int x = BC + m;
+    const int x = L.x0 + m;
     const DimConst& k = a.k;
+    // outer columns of wall corners next to an open side: one-sided
+    // tangential gradients (gradient_x_x_oneside_L0/R0 and GT_L0/GT_R0,
+    // bc_operators_wall_xy_class.f:340-360)
+    const int gt = x == 0 ? WG_L0 : (x == nx - 1 ? WG_R0 : WG_CENTRED);
     // temperature guess from u^n at the first interior node
     // (bc_operators_wall_xy_class.f:898-930, temperature_eff
-    // dim2d_prim_module.f:652-691 with centred gradients)
+    // dim2d_prim_module.f:652-691)
     double Tg;
     {
       const double r = ld(a.utmp, f, 0, x, 2);
       const double mx = ld(a.utmp, f, 1, x, 2), my = ld(a.utmp, f, 2, x, 2);
       const double E = ld(a.utmp, f, 3, x, 2);
-      const double gx = 0.5 / a.dx * (-ld(a.utmp, f, 0, x - 1, 2) + ld(a.utmp, f, 0, x + 1, 2));
+      double gx;
+      if (gt == WG_L0) gx = 1.0 / a.dx * (-ld(a.utmp, f, 0, x, 2) + ld(a.utmp, f, 0, x + 1, 2));
+      else if (gt == WG_R0) gx = 1.0 / a.dx * (-ld(a.utmp, f, 0, x - 1, 2) + ld(a.utmp, f, 0, x, 2));
+      else gx = 0.5 / a.dx * (-ld(a.utmp, f, 0, x - 1, 2) + ld(a.utmp, f, 0, x + 1, 2));
       const double gy = 0.5 / a.dy * (-ld(a.utmp, f, 0, x, 1) + ld(a.utmp, f, 0, x, 3));
       const double vx = mx / r, vy = my / r;
       const double teff = 1.0 / r * (E - 0.5 * r * (vx * vx + vy * vy) -
@@ -234,10 +284,18 @@ __host__ __device__ void node_bc_cell(const NodeBcArgs& a, int m) {
     WallRoot c;
     c.md1 = r1;
     c.md2 = r2;
-    // md_y: neighbours of the first interior node; the W/E ghosts at the
-    // ends are mirrors (applied before S in the preset's order)
-    c.my0 = x - 1 < BC ? ld(u, f, 0, mirror_lo_hi(x - 1, nx), 2) : ld(u, f, 0, x - 1, 2);
-    c.my1 = x + 1 >= nx - BC ? ld(u, f, 0, mirror_lo_hi(x + 1, nx), 2) : ld(u, f, 0, x + 1, 2);
+    // md_y: neighbours of the first interior node.  A mirror W/E ghost is
+    // read at its source (the mirror side comes before S in the presets'
+    // order and is written by this same launch); an open side's ghost
+    // column holds the stage output.  The one-sided types read one side.
+    c.my0 = c.my1 = 0.0;
+    if (gt != WG_L0)
+      c.my0 = x - 1 < BC && !a.open_w ? ld(u, f, 0, mirror_lo_hi(x - 1, nx), 2)
+                                      : ld(u, f, 0, x - 1, 2);
+    if (gt != WG_R0)
+      c.my1 = x + 1 >= nx - BC && !a.open_e ? ld(u, f, 0, mirror_lo_hi(x + 1, nx), 2)
+                                            : ld(u, f, 0, x + 1, 2);
+    c.gt = gt;
     c.vx = -my1 / r1;
     c.vy = mx1 / r1;
     c.Ed = ld(u, f, 3, x, 2);
@@ -261,11 +319,11 @@ __host__ __device__ void node_bc_cell(const NodeBcArgs& a, int m) {
     NBC_ST(&u[(size_t)0 * f.pitch + x], rg2);
     NBC_ST(&u[f.plane + (size_t)1 * f.pitch + x], mxg);
     NBC_ST(&u[2 * f.plane + (size_t)1 * f.pitch + x], myg);
-    // south corners (reflection_x of these ghost cells,
-    // bc_operators_reflection_x_class.f:236-286)
+    // south corners of a mirror side (reflection_x of these ghost cells,
+    // bc_operators_reflection_x_class.f:236-286; after S in the order)
     int cx = -1;
-    if (x < 2 * BC) cx = 2 * BC - 1 - x;
-    else if (x >= nx - 2 * BC) cx = 2 * nx - 2 * BC - 1 - x;
+    if (x < 2 * BC && !a.open_w) cx = 2 * BC - 1 - x;
+    else if (x >= nx - 2 * BC && !a.open_e) cx = 2 * nx - 2 * BC - 1 - x;
     if (cx >= 0) {
       NBC_ST(&u[(size_t)1 * f.pitch + cx], pre_x[0] * rg);
       NBC_ST(&u[(size_t)0 * f.pitch + cx], pre_x[0] * rg2);
@@ -274,16 +332,31 @@ __host__ __device__ void node_bc_cell(const NodeBcArgs& a, int m) {
     }
     return;
   }
-  m -= n_s;
-  {  // corners from the interior: pre_x * pre_y * u(mirror x, mirror y)
+  m -= L.n_s;
+  {
     const int nc = BC * BC;
-    int c = m / nc;
+    int k = m / nc;  // k-th corner with node work
     const int r = m % nc;
-    if (a.south_wall) c += 2;  // only NW (2) and NE (3)
+    int c = 0;
+    for (; c < 4; c++)
+      if (L.corners >> c & 1) {
+        if (k == 0) break;
+        k--;
+      }
+    if (c == 4) return;
     const bool east = c & 1, north = c >> 1;
     const int x = (east ? nx - BC : 0) + r % BC;
     const int y = (north ? ny - BC : 0) + r / BC;
-    const int sx = mirror_lo_hi(x, nx), sy = mirror_lo_hi(y, ny);
+    const int sx = mirror_lo_hi(x, nx);
+    if (north && a.open_n) {
+      // reflection_x of the open N ghost rows (half_wall_S_open's NW corner,
+      // last in its order): pre_x * u(mirror x, y)
+      for (int v = 0; v < 4; v++)
+        NBC_ST(&u[(size_t)v * f.plane + (size_t)y * f.pitch + x], pre_x[v] * ld(u, f, v, sx, y));
+      return;
+    }
+    // mirror corners from the interior: pre_x * pre_y * u(mirror x, mirror y)
+    const int sy = mirror_lo_hi(y, ny);
     for (int v = 0; v < 4; v++)
       NBC_ST(&u[(size_t)v * f.plane + (size_t)y * f.pitch + x], pre_x[v] * pre_y[v] * ld(u, f, v, sx, sy));
   }
@@ -310,6 +383,7 @@ __host__ __device__ __forceinline__ NodeBcArgs batch_node_args(const NodeBcBatch
   a.ymap0 = d.ymap0;
   a.south_wall = d.south_wall;
   a.corners_y = d.corners_y;
+  a.open_w = a.open_e = a.open_n = 0;
   a.status = d.status;
   a.wall = P.wall;
   a.k = P.k;

@@ -14,7 +14,8 @@ __global__ void __launch_bounds__(128) k_open_ghosts(StageArgs a) {
 }  // namespace
 
 cudaError_t launch_open_ghosts(const StageArgs& a, int mode, cudaStream_t s) {
-  const int total = open_ghost_count(a.f);
+  const int total = open_ghost_count(a.f, a.open);
+  if (total == 0) return cudaSuccess;
   const int blocks = (total + 127) / 128;
   if (mode == 0) k_open_ghosts<0><<<blocks, 128, 0, s>>>(a);
   else k_open_ghosts<1><<<blocks, 128, 0, s>>>(a);

@@ -15,6 +15,10 @@
 //     from one-sided normal gradients, incoming ones set to zero, mapped
 //     back through the conservative <- primitive Jacobian
 //     (ns_vdw2d_prim_module.f:249-893).
+// The presets that mix open sections with a south wall (wall_S_open,
+// half_wall_S_open, library_config.py:118-150) integrate only their open
+// sections (StageArgs::open mask); where an open W/E edge meets the wall
+// corner, the corner's wall flux closes the edge's first interior row.
 // One thread per ghost cell; the state is read straight from global memory
 // (the ghost ring is a few rows, L2-resident), the output is written with
 // the same RK3 stage update as the interior kernel.  Included by
@@ -94,15 +98,16 @@ __host__ __device__ __forceinline__ double tcap_at(const Frame& F, int n, int t,
   return 0.5 / r * (gn * gn + gt * gt);
 }
 
-// Face flux at the face between frame nodes a = (-1, 0) and b = (0, 0)
+// Face inputs at the face between frame nodes a = (-1, 0) and b = (0, 0)
 // with the tangential operators of mode tm (the normal operators are the
 // interior ones in every set used here: y_{L0,L1,R1,R0} change only
-// y-derivatives of x-faces, x_{...} only x-derivatives of y-faces).
-__host__ __device__ void frame_face_flux(const Frame& F, int tm, double rdn, double rdt,
-                                const DimConst& k, double out[4]) {
+// y-derivatives of x-faces, x_{...} only x-derivatives of y-faces);
+// *tcl_b = classical temperature_eff of node b.
+__host__ __device__ void frame_face_in(const Frame& F, int tm, double rdn, double rdt,
+                                       const DimConst& k, FaceIn& fi, double* tcl_b) {
   const Node a = F.node(-1, 0), b = F.node(0, 0);
   const NP pa = nprim(a, k), pb = nprim(b, k);
-  FaceIn fi;
+  *tcl_b = pb.tcl;
   fi.ra = a.r; fi.rb = b.r;
   fi.mna = a.mn; fi.mnb = b.mn;
   fi.mta = a.mt; fi.mtb = b.mt;
@@ -151,7 +156,33 @@ __host__ __device__ void frame_face_flux(const Frame& F, int tm, double rdn, dou
   fi.dunt = dunt;
   fi.dutt = dutt;
   fi.lap = d2n + d2t;
+}
+
+// Interior-formula flux at that face (flux_x/y_oneside with the set of tm)
+__host__ __device__ void frame_face_flux(const Frame& F, int tm, double rdn, double rdt,
+                                         const DimConst& k, double out[4]) {
+  FaceIn fi;
+  double tcl_b;
+  frame_face_in(F, tm, rdn, rdt, k, fi, &tcl_b);
   face_flux(fi, k, out);
+}
+
+// Wall flux at a y-face on the south wall (node b = first interior row):
+// the flux of the wall corner sections, bc_operators_wall_xy_class.f:
+// 702-854 (SW: x_oneside_L0 set in column 1, L1 in column 2; SE: R1 in
+// column nx-1, R0 in column nx) with compute_wall_flux_y,
+// wall_xy_equilibrium_module.f:445-908.  Of the set's operators the wall
+// flux uses the tangential density gradient and second derivative (mode
+// tm) and the temperature of node b with the tangential gradient of mode
+// tm (temperature_eff with gradient_x_x_oneside_L0/R0 in the outer column).
+__host__ __device__ void frame_wall_flux_s(const Frame& F, int tm, double rdn, double rdt,
+                                           double dn, double q, const DimConst& k,
+                                           double out[4]) {
+  FaceIn fi;
+  double tcl_b;
+  frame_face_in(F, tm, rdn, rdt, k, fi, &tcl_b);
+  const double tl = k.c38cv * (tcl_b - k.iwe * fi.kb);
+  wall_face_flux(fi, tl, dn, q, q, k, out);
 }
 
 // hedstrom_xy_module.f:445-558 with obc_eigenqties_bc.  q = conservative
@@ -240,30 +271,53 @@ __host__ __device__ void prim_gradient(const double* u, const Field& f, int x, i
 
 }  // namespace
 
-// number of ghost cells of a field open on all sides
-inline __host__ __device__ int open_ghost_count(const Field& f) {
-  const int ex = f.nx - 2 * BC, ey = f.ny - 2 * BC;
-  return 2 * BC * ex + 2 * BC * ey + 4 * BC * BC;
+// cells of ghost section s (0..3 = S, N, W, E edges, 4..7 = SW, SE, NW,
+// NE corners; bit s of an OPEN_* mask)
+inline __host__ __device__ int open_section_cells(const Field& f, int s) {
+  if (s < 2) return BC * (f.nx - 2 * BC);
+  if (s < 4) return BC * (f.ny - 2 * BC);
+  return BC * BC;
 }
 
-// Ghost cell number m of a field open on all sides: time derivative
+// number of ghost cells of the sections in `mask`
+inline __host__ __device__ int open_ghost_count(const Field& f, int mask) {
+  int n = 0;
+  for (int s = 0; s < 8; s++)
+    if (mask >> s & 1) n += open_section_cells(f, s);
+  return n;
+}
+
+// Ghost cell number m of the open sections a.open: time derivative
 // (mode 0) or RK stage update (mode 1) written to a.uout.  Cells are
-// numbered S edge, N edge (BC rows of ex cells each), W edge, E edge (BC
-// columns of ey cells each), then the 4 corners (SW, SE, NW, NE) of BC x BC.
+// numbered section by section in the order S edge, N edge (BC rows of ex
+// cells each), W edge, E edge (BC columns of ey cells each), SW, SE, NW,
+// NE corners (BC x BC), skipping sections outside the mask.  With a wall on
+// the south side (a.wall_s; its corner sections are wall sections), the
+// bottom y-face of the first interior row of an open W or E edge carries
+// the wall corner flux instead of the open-edge flux: the open edge's own
+// flux range starts one face higher (check_y_flux_interactions,
+// bc_operators_openbc_class.f:437-551) and the wall corner operator
+// supplies that face.
 inline __host__ __device__ void open_ghost_cell(const StageArgs& a, int m, int mode) {
   const Field f = a.f;
   const int ex = f.nx - 2 * BC, ey = f.ny - 2 * BC;  // interior extents
-  const int n_ns = BC * ex;                           // cells of one N or S edge
-  const int n_ew = BC * ey;                           // cells of one E or W edge
-  const int n_c = BC * BC;
-  if (m < 0 || m >= open_ghost_count(f)) return;
+  const int mask = a.open;
+  if (m < 0) return;
+  int sec = 0;
+  for (; sec < 8; sec++) {
+    if (!(mask >> sec & 1)) continue;
+    const int c = open_section_cells(f, sec);
+    if (m < c) break;
+    m -= c;
+  }
+  if (sec == 8) return;
   const DimConst& k = a.k;
   int x, y;
   double L[4];
   double q[4];
-  if (m < 2 * n_ns) {  // N or S edge cell: x-faces in the ghost row
-    const bool north = m >= n_ns;
-    const int r = north ? m - n_ns : m;
+  if (sec < 2) {  // N or S edge cell: x-faces in the ghost row
+    const bool north = sec == 1;
+    const int r = m;
     x = BC + r % ex;
     const int row = r / ex;  // 0 or 1
     y = north ? f.ny - BC + row : row;
@@ -284,10 +338,9 @@ inline __host__ __device__ void open_ghost_cell(const StageArgs& a, int m, int m
     // hedstrom_xy_module.f:290-303
 #pragma unroll
     for (int v = 0; v < 4; v++) L[v] = (Fl[v] - Fr[v]) * a.rdx + ch[v];
-  } else if (m < 2 * n_ns + 2 * n_ew) {  // E or W edge cell: y-faces in the ghost column
-    const int mm = m - 2 * n_ns;
-    const bool east = mm >= n_ew;
-    const int r = east ? mm - n_ew : mm;
+  } else if (sec < 4) {  // E or W edge cell: y-faces in the ghost column
+    const bool east = sec == 3;
+    const int r = m;
     y = BC + r % ey;
     const int col = r / ey;
     x = east ? f.nx - BC + col : col;
@@ -296,7 +349,11 @@ inline __host__ __device__ void open_ghost_cell(const StageArgs& a, int m, int m
     if (!east && x == 0) tm = T_L0;
     double Gb[4], Gt[4];
     Frame Fa{a.uin, f, x, y, true};
-    frame_face_flux(Fa, tm, a.rdy, a.rdx, k, Gb);
+    if (a.wall_s && y == BC)
+      frame_wall_flux_s(Fa, tm, a.rdy, a.rdx, a.dy, wall_heat_flux(a.wall, a.xmap0 + x * a.dx),
+                        k, Gb);
+    else
+      frame_face_flux(Fa, tm, a.rdy, a.rdx, k, Gb);
     Frame Fb{a.uin, f, x, y + 1, true};
     frame_face_flux(Fb, tm, a.rdy, a.rdx, k, Gt);
     double g[4], ch[4];
@@ -309,8 +366,7 @@ inline __host__ __device__ void open_ghost_cell(const StageArgs& a, int m, int m
     L[2] = ch[2] + (Gb[1] - Gt[1]) * a.rdy;
     L[3] = ch[3] + (Gb[3] - Gt[3]) * a.rdy;
   } else {  // corner cell: characteristic x + characteristic y
-    const int mm = m - 2 * n_ns - 2 * n_ew;
-    const int c = mm / n_c, r = mm % n_c;
+    const int c = sec - 4, r = m;
     const bool east = c & 1, north = c >> 1;
     x = (east ? f.nx - BC : 0) + r % BC;
     y = (north ? f.ny - BC : 0) + r / BC;

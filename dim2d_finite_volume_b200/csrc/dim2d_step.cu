@@ -31,7 +31,7 @@ StageArgs make_stage_args(const dim2d_handle* h, const double* uin, double* uout
   a.periodic = h->periodic;
   a.wall_s = h->south_wall;
   a.variant = h->variant;
-  a.open = h->open_all;
+  a.open = h->open_mask;
   a.mixed = h->precision == DIM2D_MIXED;
   a.t = h->t;
   a.xmap0 = h->xmap0;
@@ -55,6 +55,9 @@ static NodeBcArgs make_node_args(const dim2d_handle* h, const double* utmp, doub
   a.ymap0 = h->ymap0;
   a.south_wall = h->south_wall;
   a.corners_y = h->corners_y;
+  a.open_w = h->open_w;
+  a.open_e = h->open_e;
+  a.open_n = h->open_n;
   a.status = h->status;
   a.wall = h->wall;
   a.k = h->k;
@@ -127,7 +130,8 @@ cudaError_t launch_stage_work(dim2d_handle* h, const StageArgs& a, int mode) {
 static int stage(dim2d_handle* h, int st, const double* uin, double* uout, double dt) {
   // on open fields every ghost cell has a time derivative and is integrated
   // like the interior (x/y_borders widened, field_abstract_class.f:244-270)
-  // and no node boundary pass follows
+  // and no node boundary pass follows; the mixed presets integrate their
+  // open sections and run the node pass for the others
   cudaError_t e = launch_stage_work(h, make_stage_args(h, uin, uout, dt, st), 1);
   if (e != cudaSuccess) return cuda_error(e, "rk3 stage");
   if (h->periodic || h->open_all) return DIM2D_OK;  // periodic images: by the stage kernel

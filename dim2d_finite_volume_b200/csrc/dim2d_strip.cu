@@ -26,8 +26,8 @@
 // Warps are independent (__syncwarp only), so the latency of one warp's
 // loads is hidden by the arithmetic of the others.
 //
-// On a field open on all sides the launch also integrates the ghost cells
-// (open_ghost_cell, one thread each): they take the first CTAs of the
+// On a field with open sections the launch also integrates their ghost
+// cells (open_ghost_cell, one thread each): they take the first CTAs of the
 // grid, so their long dependent chains start first and overlap the strips.
 // Ghost and interior cells read the same input and write disjoint cells.
 #include "dim2d_open.cuh"
@@ -374,7 +374,9 @@ __device__ __forceinline__ void y_face_mix(const StageArgs& a, const FluxCoefF& 
 }
 
 // boundary kinds of the strip kernel
-enum StripKind : int { K_PLAIN = 0, K_WALL = 1, K_OPEN = 2 };
+// K_WALL_OPEN: open sections and a south wall (wall_S_open,
+// half_wall_S_open): ghost CTAs of the open sections, wall faces in the strips
+enum StripKind : int { K_PLAIN = 0, K_WALL = 1, K_OPEN = 2, K_WALL_OPEN = 3 };
 
 // grid: [ghost CTAs (K_OPEN only)] + sx * sy strip CTAs, x fastest
 // The work of strip CTA number b of one field (sx strips per row band).
@@ -539,14 +541,14 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
 template <int H, int WPC, int MINB, int MODE, int KIND, bool MIX>
 __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost_ctas, int sx) {
   int b = blockIdx.x;
-  if (KIND == K_OPEN) {
+  if (KIND == K_OPEN || KIND == K_WALL_OPEN) {
     if (b < ghost_ctas) {
       open_ghost_cell(a, b * (32 * WPC) + threadIdx.x, MODE);
       return;
     }
     b -= ghost_ctas;
   }
-  strip_cta<H, WPC, MODE, KIND == K_WALL, MIX>(a, b, sx);
+  strip_cta<H, WPC, MODE, KIND == K_WALL || KIND == K_WALL_OPEN, MIX>(a, b, sx);
 }
 
 // stage arguments of domain i of a batched launch
@@ -600,7 +602,8 @@ __global__ void __launch_bounds__(32 * WPC, MINB)
   if (KIND == K_OPEN) {
     if (b < P.ghost_ctas) {
       const int i = batch_domain<true>(P, b);
-      const StageArgs a = batch_stage_args(P, i);
+      StageArgs a = batch_stage_args(P, i);
+      a.open = OPEN_ALL;
       open_ghost_cell(a, (b - P.d[i].ghost0) * (32 * WPC) + threadIdx.x, 1);
       return;
     }
@@ -621,6 +624,7 @@ template <int H, int WPC, int MINB, int MODE, bool MIX>
 const void* strip_fn(int kind) {
   if (kind == K_WALL) return (const void*)k_strip<H, WPC, MINB, MODE, K_WALL, MIX>;
   if (kind == K_OPEN) return (const void*)k_strip<H, WPC, MINB, MODE, K_OPEN, MIX>;
+  if (kind == K_WALL_OPEN) return (const void*)k_strip<H, WPC, MINB, MODE, K_WALL_OPEN, MIX>;
   return (const void*)k_strip<H, WPC, MINB, MODE, K_PLAIN, MIX>;
 }
 
@@ -629,7 +633,7 @@ cudaError_t launch_strip_shape(const StageArgs& a, int mode, cudaStream_t s) {
   const size_t smem =
       (size_t)WPC * (a.mixed ? WARP_DOUBLES_MIX : WARP_DOUBLES) * sizeof(double);
   const bool wall = a.wall_w || a.wall_e || a.wall_s || a.wall_n;
-  const int kind = a.open ? K_OPEN : (wall ? K_WALL : K_PLAIN);
+  const int kind = a.open ? (wall ? K_WALL_OPEN : K_OPEN) : (wall ? K_WALL : K_PLAIN);
   const void* fn = a.mixed ? (mode == 0 ? strip_fn<H, WPC, MINB, 0, true>(kind)
                                         : strip_fn<H, WPC, MINB, 1, true>(kind))
                            : (mode == 0 ? strip_fn<H, WPC, MINB, 0, false>(kind)
@@ -638,7 +642,7 @@ cudaError_t launch_strip_shape(const StageArgs& a, int mode, cudaStream_t s) {
   if (e != cudaSuccess) return e;
   int sx = (a.f.nx - 2 * BC + SW - 1) / SW;
   const int sy = (a.f.ny - 2 * BC + H * WPC - 1) / (H * WPC);
-  int ghost_ctas = kind == K_OPEN ? (open_ghost_count(a.f) + 32 * WPC - 1) / (32 * WPC) : 0;
+  int ghost_ctas = a.open ? (open_ghost_count(a.f, a.open) + 32 * WPC - 1) / (32 * WPC) : 0;
   const unsigned blocks = (unsigned)ghost_ctas + (unsigned)sx * (unsigned)sy;
   StageArgs aa = a;
   void* args[] = {&aa, &ghost_ctas, &sx};
@@ -666,7 +670,7 @@ cudaError_t launch_strip_batch_shape(BatchStageArgs& P, int kind, bool mixed, cu
     const int sy = (d.f.ny - 2 * BC + H * WPC - 1) / (H * WPC);
     d.ghost0 = (int)ghost;
     d.strip0 = (int)strips;
-    if (kind == BK_OPEN) ghost += (open_ghost_count(d.f) + 32 * WPC - 1) / (32 * WPC);
+    if (kind == BK_OPEN) ghost += (open_ghost_count(d.f, OPEN_ALL) + 32 * WPC - 1) / (32 * WPC);
     strips += (long long)d.sx * sy;
   }
   if (ghost + strips > 0x7fffffffLL) return cudaErrorInvalidValue;

@@ -78,6 +78,14 @@ def _preset(name):
         ch = dict(N=REFLECTION_Y, S=WALL, E=REFLECTION_X, W=REFLECTION_X, NE=REFLECTION_X,
                   NW=REFLECTION_X, SE=REFLECTION_X, SW=REFLECTION_X)
         order = ["W", "E", "S", "N", "SW", "SE", "NW", "NE"]
+    elif name == "wall_S_open":  # library_config.py:118-131
+        ch = dict(N=HEDSTROM, S=WALL, E=HEDSTROM, W=HEDSTROM, NE=HEDSTROM, NW=HEDSTROM,
+                  SE=WALL, SW=WALL)
+        order = ["SW", "S", "SE", "W", "E", "NW", "N", "NE"]
+    elif name == "half_wall_S_open":  # library_config.py:134-150, the reference's default
+        ch = dict(N=HEDSTROM, S=WALL, E=HEDSTROM, W=REFLECTION_X, NE=HEDSTROM,
+                  NW=REFLECTION_X, SE=WALL, SW=REFLECTION_X)
+        order = ["W", "S", "SE", "SW", "E", "N", "NE", "NW"]
     elif name == "reflection_xy":
         ch = dict(N=REFLECTION_Y, S=REFLECTION_Y, E=REFLECTION_X, W=REFLECTION_X,
                   NE=REFLECTION_Y, NW=REFLECTION_Y, SE=REFLECTION_Y, SW=REFLECTION_Y)

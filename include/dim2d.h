@@ -125,6 +125,13 @@ DIM2D_API void dim2d_default_params(dim2d_params *p);
  * PERIODIC_Y on N/S and PERIODIC_X elsewhere (library_config.py:72-87),
  * all types DIM2D_BC_NODES; it selects the periodic_xy operator
  * (src/boundary_conditions/periodic_xy/bc_operators_class.f:116-199).
+ * The other accepted configurations are the reference's presets
+ * (library_config.py:58-150): hedstrom_xy, reflection_xy,
+ * wall_S_reflection, wall_S_open and half_wall_S_open, each with the
+ * types its choices imply (reflection: BC_NODES, wall: BC_FLUX_AND_NODE,
+ * hedstrom: BC_TIMEDEV); anything else returns DIM2D_ERR_UNSUPPORTED, as
+ * does a half_wall_S_open bc_order with the S edge before the W edge or
+ * the SW corner before the S edge.
  * Allocates three device copies of the field.
  * Replaces: field%ini + td_integrator selection (field_abstract_class.f:148-198). */
 DIM2D_API int dim2d_create(const dim2d_params *p, int nx, int ny, const int bc_choice[8],
@@ -243,7 +250,9 @@ DIM2D_API int dim2d_step_noalloc(const dim2d_params *p, int nx, int ny, const in
  * Members are fields created with dim2d_create and uploaded, on the
  * batch's device, sharing one dim2d_params (FP64 and DIM2D_MIXED fields
  * form separate groups); the batch borrows their
- * buffers and advances their state and time.  While a field is a member,
+ * buffers and advances their state and time.  wall_S_open and
+ * half_wall_S_open fields cannot join a batch (DIM2D_ERR_UNSUPPORTED).
+ * While a field is a member,
  * dim2d_step on it is refused; dim2d_download/dim2d_time_dev of a member
  * are ordered after the batch's queued steps.  dim2d_destroy of a member
  * removes it first. */

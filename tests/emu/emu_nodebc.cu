@@ -31,9 +31,9 @@ static inline void emu_store(double* p, double v) {
 using namespace dim2d;
 int main(int argc, char** argv) {
   FILE* fi = fopen(argv[1], "rb");
-  int hdr[4];  // nx, ny, south_wall, corners_y
+  int hdr[7];  // nx, ny, south_wall, corners_y, open_w, open_e, open_n
   double par[10];  // dx, dy, re, we, pr, cv_r, viscous_r, cos_angle, xmap0, qconst
-  if (fread(hdr, 4, 4, fi) != 4 || fread(par, 8, 10, fi) != 10) return 2;
+  if (fread(hdr, 4, 7, fi) != 7 || fread(par, 8, 10, fi) != 10) return 2;
   const int nx = hdr[0], ny = hdr[1];
   const size_t plane = (size_t)nx * ny;
   std::vector<double> ut(4 * plane), u(4 * plane);
@@ -48,6 +48,7 @@ int main(int argc, char** argv) {
   a.f.nx = nx; a.f.ny = ny; a.f.pitch = nx; a.f.plane = plane;
   a.dx = par[0]; a.dy = par[1]; a.rdx = 1.0 / par[0]; a.rdy = 1.0 / par[1];
   a.south_wall = hdr[2]; a.corners_y = hdr[3];
+  a.open_w = hdr[4]; a.open_e = hdr[5]; a.open_n = hdr[6];
   unsigned int status = 0; a.status = &status;
   DimConst& k = a.k;
   k.re = par[2]; k.we = par[3]; k.pr = par[4]; k.cv_r = par[5]; k.viscous_r = par[6];

@@ -23,7 +23,15 @@ int main(int argc, char** argv) {
   a.f.nx = nx; a.f.ny = ny; a.f.pitch = nx; a.f.plane = plane; a.rdx = 1.0 / dx; a.rdy = 1.0 / dy; a.dx = dx; a.dy = dy;
   DimConst& k = a.k; k.re = par[0]; k.we = par[1]; k.pr = par[2]; k.cv_r = par[3]; k.viscous_r = par[4];
   k.ire = 1.0 / k.re; k.iwe = 1.0 / k.we; k.ipr = 1.0 / k.pr; k.irepr = 1.0 / (k.re * k.pr); k.c15cv = 1.5 / k.cv_r; k.c3cv = 3.0 / k.cv_r; k.two_mu = 2.0 + k.viscous_r;
-  int total = open_ghost_count(a.f);
+  k.c38cv = 3.0 / (8.0 * k.cv_r);
+  // optional: open-section mask, south wall flag, x_map(1), constant wall heat flux
+  a.open = argc > 3 ? atoi(argv[3]) : OPEN_ALL;
+  a.wall_s = argc > 4 ? atoi(argv[4]) : 0;
+  a.xmap0 = argc > 5 ? atof(argv[5]) : 0.0;
+  const double qc = argc > 6 ? atof(argv[6]) : 0.0;
+  a.wall.cos_angle = argc > 7 ? atof(argv[7]) : 0.0;
+  a.wall.heat_choice = qc != 0.0 ? 1 : 0; a.wall.qmax = qc;
+  int total = open_ghost_count(a.f, a.open);
   for (int m = -3; m < total + 300; m++) open_ghost_cell(a, m, 0);
   long guard = 0; for (size_t i = 0; i < 4 * plane; i++) { if (out[i] != -777.0) guard++; if (out[8 * plane + i] != -777.0) guard++; }
   long written = 0; for (size_t i = 4 * plane; i < 8 * plane; i++) if (out[i] != -777.0) written++;

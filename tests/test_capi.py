@@ -59,3 +59,38 @@ def test_host_only_calls_without_gpu():
     with pytest.raises(F.Dim2dError) as e:
         F._check(F.library().dim2d_ini_coordinates(3, 12, 0, 1, 0, 1, F._ptr(x), F._ptr(y)))
     assert e.value.code == 1
+
+
+def test_mixed_presets_classified_before_any_device_call():
+    """wall_S_open and half_wall_S_open are provided configurations; a
+    half_wall_S_open section order whose node pass the kernels do not
+    reproduce (S wall before the W mirror) is refused with its own message.
+    Classification happens before any CUDA call, so this runs without a GPU."""
+    import ctypes
+
+    from dim2d_finite_volume_b200 import field as F
+    L = F.library()
+    arr = ctypes.c_int * 8
+    p = F.default_params()
+    h = ctypes.c_void_p()
+    for preset in ("wall_S_open", "half_wall_S_open"):
+        ch, ty, order = F._preset(preset)
+        rc = L.dim2d_create(ctypes.byref(p), 40, 30, arr(*ch), arr(*ty), arr(*order), 0,
+                            ctypes.byref(h))
+        msg = L.dim2d_last_error().decode()
+        assert "not provided" not in msg and "half_wall_S_open needs" not in msg, (preset, msg)
+        if rc == 0:  # a device is present
+            L.dim2d_destroy(h)
+    ch, ty, order = F._preset("half_wall_S_open")
+    bad = list(order)
+    i, j = bad.index(F._SECTION["W"]), bad.index(F._SECTION["S"])
+    bad[i], bad[j] = bad[j], bad[i]
+    rc = L.dim2d_create(ctypes.byref(p), 40, 30, arr(*ch), arr(*ty), arr(*bad), 0, ctypes.byref(h))
+    assert rc != 0 and "half_wall_S_open needs" in L.dim2d_last_error().decode()
+    # a W side that is neither open nor a mirror beside the open N/E sides
+    ch2 = list(ch)
+    ch2[3] = F.WALL
+    ty2 = [F.bc_type_of(c) for c in ch2]
+    rc = L.dim2d_create(ctypes.byref(p), 40, 30, arr(*ch2), arr(*ty2), arr(*order), 0,
+                        ctypes.byref(h))
+    assert rc != 0 and "not provided" in L.dim2d_last_error().decode()

@@ -45,9 +45,32 @@ def defined_ghost_mask(nx, ny, south_wall):
     return m
 
 
+# (south_wall, corners_y, open_w, open_e, open_n) of the node pass per preset
+FLAGS = {"wall_S_reflection": (1, 0, 0, 0, 0), "reflection_xy": (0, 1, 0, 0, 0),
+         "wall_S_open": (1, 0, 1, 1, 1), "half_wall_S_open": (1, 0, 0, 1, 1)}
+
+
+def node_ghosts(nx, ny, preset):
+    """Ghost cells that have node work (the others are stage output)."""
+    g = np.zeros((ny, nx), bool)
+    south_wall, _, open_w, open_e, open_n = FLAGS[preset]
+    g[:2, :] = True  # S side: wall or mirror, corners included
+    if not open_n:
+        g[-2:, :] = True
+    if not open_w:
+        g[:, :2] = True
+    if not open_e:
+        g[:, -2:] = True
+    return g
+
+
 @pytest.mark.parametrize("preset,n,ny,seed", [("wall_S_reflection", 40, 30, 1),
                                                ("wall_S_reflection", 9, 12, 2),
-                                               ("reflection_xy", 33, 21, 3)])
+                                               ("reflection_xy", 33, 21, 3),
+                                               ("wall_S_open", 40, 30, 4),
+                                               ("wall_S_open", 9, 12, 5),
+                                               ("half_wall_S_open", 40, 30, 6),
+                                               ("half_wall_S_open", 11, 9, 7)])
 def test_node_bc_host_emulation(oracle, emu, preset, n, ny, seed):
     from dim2d_finite_volume_b200 import field as F, ic
     exe, d = emu
@@ -59,17 +82,16 @@ def test_node_bc_host_emulation(oracle, emu, preset, n, ny, seed):
     oracle.apply_bc_on_nodes(cfg, 0.0, x_map, y_map, un.copy(), un)  # u^n as ini leaves it
     rng = np.random.default_rng(seed)
     u = un * (1.0 + 1e-3 * rng.standard_normal(un.shape))       # a stage state
-    u[:, :2, :] = u[:, -2:, :] = 1e31                             # ghosts: stage-1 garbage
-    u[:, :, :2] = u[:, :, -2:] = 1e31
+    u[:, node_ghosts(nx, nyy, preset)] = 1e31                     # ghosts: stage-1 garbage
     want = u.copy()
     oracle.lib().orc_clear_status()
     oracle.apply_bc_on_nodes(cfg, 0.0, x_map, y_map, un, want)
     assert oracle.lib().orc_status() == 0
-    south_wall = int(preset == "wall_S_reflection")
+    south_wall = FLAGS[preset][0]
     p = oracle.get_params()
     fin, fout = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
     with open(fin, "wb") as fh:
-        np.array([nx, nyy, south_wall, int(preset == "reflection_xy")], dtype=np.int32).tofile(fh)
+        np.array([nx, nyy, *FLAGS[preset]], dtype=np.int32).tofile(fh)
         np.array([dx, y_map[1] - y_map[0], p.re, p.we, p.pr, p.cv_r, p.viscous_r,
                   np.cos(p.wall_micro_contact_angle * np.arccos(-1.0) / 180.0), x_map[0],
                   0.0]).tofile(fh)
@@ -81,6 +103,8 @@ def test_node_bc_host_emulation(oracle, emu, preset, n, ny, seed):
     got = np.fromfile(fout).reshape(4, nyy, nx)
     mask = defined_ghost_mask(nx, nyy, south_wall)
     assert np.array_equal(got[:, 2:-2, 2:-2], u[:, 2:-2, 2:-2])  # interior untouched
+    stage_cells = ~node_ghosts(nx, nyy, preset)
+    assert np.array_equal(got[:, stage_cells], u[:, stage_cells])  # open sections untouched
     wall_rows = np.zeros_like(mask)
     if south_wall:
         wall_rows[:, :2, :] = True
