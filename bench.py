@@ -331,14 +331,16 @@ def run_served(a):
     from dim2d_finite_volume_b200 import server as Sm
     from dim2d_finite_volume_b200 import workloads
     reqs = workloads.served_requests(a.seed + 99, a.served, rate=50.0)
-    with Sm.Server(chunk_steps=500) as srv:
+    with Sm.Server(params=workloads.served_params(), chunk_steps=500) as srv:
         run = Sm.serve(srv, reqs)
     lat = np.array(run["latencies"])
     return {
         "workload": "served stream: %d requests, Poisson arrivals at 50/s, n log-uniform in "
                     "[64,1024], steps uniform in [500,20000], T0 in [0.90,0.99], wall "
-                    "(wall_S_reflection) / open, FP64 or mixed precision per request (%d mixed)"
-                    % (len(reqs), sum(r["precision"] for r in reqs)),
+                    "(wall_S_reflection) / open, FP64 or mixed precision per request (%d mixed); "
+                    "one bubble per request with the equilibrium interface width at T0, "
+                    "We = %g for the whole stream"
+                    % (len(reqs), sum(r["precision"] for r in reqs), workloads.SERVED_WE),
         "value": run["cell_updates"] / run["wall_s"], "unit": "cell-updates/s",
         "wall_s": run["wall_s"], "cell_updates": int(run["cell_updates"]),
         "latency_p50_s": float(np.percentile(lat, 50)),
@@ -348,11 +350,12 @@ def run_served(a):
         "max_active": int(run["stats"]["max_active"]),
         "failed_requests": len(run["failed"]),
         "nonfinite_requests": len(run["nonfinite"]),
-        "failed_note": "requests whose bubble collapses and the solve blows up (the seeded "
-                       "saturated-density bubble is not in Laplace equilibrium): wall "
-                       "requests stop at the wall ghost-cell root as the reference does "
-                       "(the oracle fails on the same inputs), others end non-finite; "
-                       "their latency and cell-updates are still counted",
+        "failed_note": "failed = the wall ghost-cell root was not found (where the reference "
+                       "stops); non-finite = the solve blew up.  Open (Hedstrom) requests on "
+                       "small grids run long in physical time and meet the reference's "
+                       "open-boundary instability (velocity in the outermost ghost layer "
+                       "growing ~20x per unit time whatever the time step; the oracle blows up "
+                       "on the same inputs); their latency and cell-updates are still counted",
         "timing": "host wall clock from the first arrival to the last completion (the "
                   "stream is replayed in real time); latency = submit to completion",
     }
@@ -370,7 +373,8 @@ def run_mixed(a, stream, F, torch):
     cells = (nx - 4) * (ny - 4)
     flds = {}
     for prec in (F.MIXED, F.FP64):
-        fld = F.Field(nx, ny, bc="wall_S_reflection", precision=prec)
+        fld = F.Field(nx, ny, bc="wall_S_reflection", precision=prec,
+                      params=workloads.mixed_params())
         fld.set_stream(stream.cuda_stream)
         fld.ini(d["nodes"], d["x_map"], d["y_map"])
         fld.apply_bc_on_nodes()  # field%ini
@@ -414,7 +418,8 @@ def run_mixed(a, stream, F, torch):
     vd = cells * done / (ms[F.FP64] * 1e-3) if done else None
     return {
         "workload": "mixed precision %d^2: %d bubbles r in [0.05,0.1], T0=0.97, wall "
-                    "(wall_S_reflection), %d steps" % (a.mixed_n, len(d["bubbles"]), a.mixed_steps),
+                    "(wall_S_reflection), %d steps; equilibrium interface width at T0, We = %g"
+                    % (a.mixed_n, len(d["bubbles"]), a.mixed_steps, workloads.MIXED_WE),
         "value": vm, "unit": "cell-updates/s", "fp64_value": vd,
         "vs_fp64": (vm / vd) if vm and vd else None, "steps_run": done, "status": status,
         "errors_vs_fp64": errors, "error_bar": 1e-5,

@@ -86,6 +86,14 @@ def sound_speed(rho, mx, my, E, cv_r):
     return np.sqrt(3.0) * rho / (a * d)
 
 
+def interface_length(T, we):
+    """Equilibrium width of the liquid-vapour interface at temperature T
+    (dim2d_state_eq_module.f:90-125, high-temperature branch): the width the
+    reference's own bubble initial conditions use (e.g.
+    dim2d_ic/bubble_next_to_wall/ic_class.f:186)."""
+    return 1.0 / math.sqrt(2.0 * we) * (1.6309400153322933 / math.sqrt(1.0 - T))
+
+
 def bubbles(x_map, y_map, T0, bubbles_xyr, li, velocity=(0.0, 0.0), we=10.0, cv_r=2.5,
             densities=None):
     """Vapour bubbles (centre x, centre y, radius) in saturated liquid.

@@ -44,16 +44,19 @@ def fill_periodic_ghosts(q):
     return q
 
 
-def domain(n, ny=None, T0=0.95, bubbles=((0.0, 0.0, 0.1),), mach=0.0, bc="periodic_xy"):
+def domain(n, ny=None, T0=0.95, bubbles=((0.0, 0.0, 0.1),), mach=0.0, bc="periodic_xy",
+           li=None, we=10.0):
     """One field: dict(nx, ny, x_map, y_map, nodes (4, ny, nx), dt, bc, T0, mach).
-    Mirror and wall fields still need their node boundary pass
+    Interface width li (default 4 dx) and Weber number we of the initial
+    energy.  Mirror and wall fields still need their node boundary pass
     (Field.apply_bc_on_nodes) after upload, as field%ini does."""
     ny = n if ny is None else ny
     nx, nyy, x_map, y_map = ic.grid(n, ny)
     dx = x_map[1] - x_map[0]
     dy = y_map[1] - y_map[0]
     u0 = mach * liquid_sound_speed(T0) if mach else 0.0
-    q = ic.bubbles(x_map, y_map, T0, list(bubbles), li=4.0 * dx, velocity=(u0, 0.0))
+    q = ic.bubbles(x_map, y_map, T0, list(bubbles), li=4.0 * dx if li is None else li,
+                   velocity=(u0, 0.0), we=we)
     if bc == "periodic_xy":
         fill_periodic_ghosts(q)
     q = np.ascontiguousarray(q)
@@ -97,6 +100,19 @@ def batched_domains(seed, count=64, sizes=tuple(range(128, 513, 64))):
 
 
 SERVED_KINDS = ("wall_S_reflection", "hedstrom_xy")
+# Weber number of the served stream: one constant set for the whole stream
+# (requests share batched launches), large enough that the equilibrium
+# interface width (0.08-0.26 over T0 in [0.9, 0.99]) fits the bubbles
+SERVED_WE = 2000.0
+
+
+def served_params():
+    """dim2d_params of the served stream: the test constant set with
+    We = SERVED_WE."""
+    from .field import default_params
+    p = default_params()
+    p.we = SERVED_WE
+    return p
 
 
 def served_requests(seed, count, rate=50.0, n_range=(64, 1024), steps_range=(500, 20000),
@@ -106,7 +122,10 @@ def served_requests(seed, count, rate=50.0, n_range=(64, 1024), steps_range=(500
     T0 in U[0.9, 0.99], wall or open boundaries, one bubble of radius in
     U[0.05, 0.2] (open fields: Mach in U[0, 0.1]), FP64 or mixed precision
     (a `mixed_fraction` share, drawn from a separate seeded stream).  Each
-    request carries its arrival time (s) from the start of the stream."""
+    request carries its arrival time (s) from the start of the stream.
+    The bubbles have the equilibrium interface width at T0 for We =
+    SERVED_WE (ic.interface_length), as the reference's bubble initial
+    conditions do; solve them with served_params()."""
     rng = np.random.default_rng(seed)
     rng_p = np.random.default_rng(seed + 7919)
     t = 0.0
@@ -120,17 +139,33 @@ def served_requests(seed, count, rate=50.0, n_range=(64, 1024), steps_range=(500
         r = float(rng.uniform(0.05, 0.2))
         bc = SERVED_KINDS[int(rng.integers(0, len(SERVED_KINDS)))]
         mach = float(rng.uniform(0.0, 0.1)) if bc == "hedstrom_xy" else 0.0
-        d = domain(n, T0=T0, bubbles=[(0.0, 0.0, r)], mach=mach, bc=bc)
+        d = domain(n, T0=T0, bubbles=[(0.0, 0.0, r)], mach=mach, bc=bc,
+                   li=ic.interface_length(T0, SERVED_WE), we=SERVED_WE)
         d.update(arrival=t, nsteps=steps, radius=r,
                  precision=1 if rng_p.uniform() < mixed_fraction else 0)
         out.append(d)
     return out
 
 
+# Weber number of the mixed-precision configuration: equilibrium interface
+# width 0.067 at T0 = 0.97, below the bubble radii
+MIXED_WE = 1.0e4
+
+
+def mixed_params():
+    """dim2d_params of the mixed-precision configuration (We = MIXED_WE)."""
+    from .field import default_params
+    p = default_params()
+    p.we = MIXED_WE
+    return p
+
+
 def mixed_2048(seed, n=2048, count=4):
     """Mixed-precision configuration: 2048^2, `count` bubbles of radius in
     U[0.05, 0.1] at seeded non-overlapping centres (clear of the walls), in
-    liquid at T0 = 0.97, wall boundaries (wall_S_reflection), at rest."""
+    liquid at T0 = 0.97, wall boundaries (wall_S_reflection), at rest.  The
+    bubbles have the equilibrium interface width at T0 for We = MIXED_WE
+    (ic.interface_length); solve them with mixed_params()."""
     rng = np.random.default_rng(seed)
     bub = []
     while len(bub) < count:
@@ -138,6 +173,7 @@ def mixed_2048(seed, n=2048, count=4):
         cx, cy = (float(v) for v in rng.uniform(-0.5 + r + 0.05, 0.5 - r - 0.05, 2))
         if all((cx - x) ** 2 + (cy - y) ** 2 > (r + rr + 0.05) ** 2 for x, y, rr in bub):
             bub.append((cx, cy, r))
-    d = domain(n, T0=0.97, bubbles=bub, mach=0.0, bc="wall_S_reflection")
+    d = domain(n, T0=0.97, bubbles=bub, mach=0.0, bc="wall_S_reflection",
+               li=ic.interface_length(0.97, MIXED_WE), we=MIXED_WE)
     d["bubbles"] = bub
     return d

@@ -32,8 +32,14 @@ def _requests(count, seed, n_range=(36, 110)):
                                      steps_range=(20, 90))
 
 
+def _params():
+    from dim2d_finite_volume_b200 import workloads
+    return workloads.served_params()
+
+
 def _alone(F, r):
-    with F.Field(r["nx"], r["ny"], bc=r["bc"], precision=r.get("precision", 0)) as fld:
+    with F.Field(r["nx"], r["ny"], bc=r["bc"], precision=r.get("precision", 0),
+                 params=_params()) as fld:
         fld.variant = 2
         fld.ini(r["nodes"], r["x_map"], r["y_map"])
         if r["bc"] != "hedstrom_xy":
@@ -56,7 +62,7 @@ def _bar(r):
 
 def test_results_same_alone_and_in_the_mix(F, S):
     reqs = _requests(8, seed=21)
-    with S.Server(chunk_steps=16) as srv:
+    with S.Server(params=_params(), chunk_steps=16) as srv:
         run = S.serve(srv, reqs, keep_results=True)
     assert run["stats"]["completed"] == len(reqs)
     assert run["failed"] == []
@@ -75,7 +81,7 @@ def test_admission_by_memory_budget(F, S):
     for r in reqs:
         r["arrival"] = 0.0  # all at once
     one = 3 * 4 * reqs[0]["ny"] * ((reqs[0]["nx"] + 15) // 16 * 16) * 8
-    with S.Server(mem_budget=2 * one + 65536, chunk_steps=10) as srv:
+    with S.Server(params=_params(), mem_budget=2 * one + 65536, chunk_steps=10) as srv:
         run = S.serve(srv, reqs, keep_results=True)
         st = srv.stats()
     assert st["completed"] == len(reqs)
@@ -89,7 +95,7 @@ def test_admission_by_memory_budget(F, S):
 def test_result_protocol(F, S):
     reqs = _requests(1, seed=2)
     r = reqs[0]
-    with S.Server(chunk_steps=8) as srv:
+    with S.Server(params=_params(), chunk_steps=8) as srv:
         rid = srv.submit(r["nodes"], r["x_map"], r["y_map"], r["dt"], r["nsteps"], r["bc"])
         assert srv.result(rid) is None  # not run yet
         while srv.stats()["completed"] < 1:
@@ -101,5 +107,5 @@ def test_result_protocol(F, S):
             srv.result(rid)  # forgotten once read
         with pytest.raises(F.Dim2dError):  # larger than the whole budget
             big = np.zeros((4, 600, 600))
-            S.Server(mem_budget=1 << 20).submit(big, np.linspace(0, 1, 600),
+            S.Server(params=_params(), mem_budget=1 << 20).submit(big, np.linspace(0, 1, 600),
                                                 np.linspace(0, 1, 600), 1e-6, 10)
