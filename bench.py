@@ -60,6 +60,8 @@ def parse():
                     help="stage-kernel variant 0..5, or 'auto' (the library's autotuner)")
     ap.add_argument("--batch-domains", type=int, default=64,
                     help="domains of the batched workload (0: skip it)")
+    ap.add_argument("--batch-mixed", type=int, default=1,
+                    help="also time the batched workload in mixed precision (0: skip it)")
     ap.add_argument("--mixed-steps", type=int, default=10000,
                     help="steps of the mixed-precision configuration (0: skip it)")
     ap.add_argument("--mixed-n", type=int, default=2048)
@@ -316,12 +318,63 @@ def run_batched(a, stream, barrier, F, torch, flush):
     launches = bt.launches - n0
     batch_ms = sum(x.elapsed_time(y) for x, y in ev)
     bt.close()
+    total_steps = 3 + steps + 3 + a.steps  # every step the FP64 fields took
+    out = {"cells_per_step": int(cells), "steps": a.steps, "batch_ms": batch_ms,
+           "plain_ms": plain_ms, "plain_steps": steps, "launches": int(launches),
+           "domains": len(doms), "shapes": shapes,
+           "kinds": {k: sum(1 for d in doms if d["bc"] == k) for k in workloads.BATCH_KINDS}}
+    if a.batch_mixed:
+        out["mixed"] = run_batched_mixed(a, stream, barrier, F, Bm, torch, flush, doms, fields,
+                                         total_steps)
     for fld in fields:
         fld.close()
-    kinds = {k: sum(1 for d in doms if d["bc"] == k) for k in workloads.BATCH_KINDS}
-    return {"cells_per_step": int(cells), "steps": a.steps, "batch_ms": batch_ms,
-            "plain_ms": plain_ms, "plain_steps": steps, "launches": int(launches),
-            "domains": len(doms), "kinds": kinds, "shapes": shapes}
+    return out
+
+
+def run_batched_mixed(a, stream, barrier, F, Bm, torch, flush, doms, fields64, total_steps):
+    """The same domains as DIM2D_MIXED fields in one batch: timed like the
+    FP64 batch, then advanced to the FP64 fields' step count and compared
+    with them (normwise over each interior, max over domains; the FP64
+    batch matches the oracle to 1e-10 in the parity tests)."""
+    fields = []
+    for d in doms:
+        fld = F.Field(d["nx"], d["ny"], bc=d["bc"], precision=F.MIXED)
+        fld.set_stream(stream.cuda_stream)
+        fld.ini(d["nodes"], d["x_map"], d["y_map"])
+        if d["bc"] not in ("periodic_xy", "hedstrom_xy"):
+            fld.apply_bc_on_nodes()  # field%ini
+        fields.append(fld)
+    bt = Bm.Batch()
+    bt.set_stream(stream.cuda_stream)
+    for fld, d in zip(fields, doms):
+        bt.add(fld, d["dt"])
+    shapes, _ = bt.autotune()
+    warm = total_steps - a.steps
+    bt.step(warm)
+    barrier()
+    n0 = bt.launches
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(a.steps)]
+    with torch.cuda.stream(stream):
+        for k in range(a.steps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            bt.step(1)
+            ev[k][1].record(stream)
+    barrier()
+    bt.sync()
+    launches = bt.launches - n0
+    ms = sum(x.elapsed_time(y) for x, y in ev)
+    bt.close()
+    err = np.zeros(4)
+    for fm, f64 in zip(fields, fields64):
+        qm, qd = fm.download(), f64.download()
+        for v in range(4):
+            b_ = qd[v, 2:-2, 2:-2]
+            err[v] = max(err[v], float(np.abs(qm[v, 2:-2, 2:-2] - b_).max() / np.abs(b_).max()))
+        fm.close()
+    return {"batch_ms": ms, "steps": a.steps, "launches": int(launches), "shapes": shapes,
+            "steps_compared": total_steps, "rel_err_vs_fp64": [float(e) for e in err]}
 
 
 def run_served(a):
@@ -555,6 +608,26 @@ def main():
                       "graph); plain: the same fields stepped one after another, each by its "
                       "own step graph; L2 flushed between steps",
         }
+        if "mixed" in bres:
+            bm = bres["mixed"]
+            tm = reduce_max([bm["batch_ms"]], dist, "cuda")[0]
+            mv = whole_job_rate(bres["cells_per_step"], world, bm["steps"], tm)
+            batched["mixed"] = {
+                "workload": "the same domains as DIM2D_MIXED fields (FP32 face pass, FP64 node "
+                            "pass / capillary third derivative / RK accumulation), one batch",
+                "value": mv, "unit": "cell-updates/s", "ms_per_step": tm / bm["steps"],
+                "steps": bm["steps"], "gpu_launches": bm["launches"], "shapes": bm["shapes"],
+                "vs_fp64_batched": mv / bv, "vs_plain_per_field": mv / pv,
+                "roofline": {"bound": "hbm", "achieved": mv * BYTES_PER_CELL_UPDATE / 1e9,
+                             "peak": peak_b, "unit": "GB/s",
+                             "frac": mv * BYTES_PER_CELL_UPDATE / 1e9 / peak_b},
+                "rel_err_vs_fp64": bm["rel_err_vs_fp64"],
+                "error_bar": 1e-5,
+                "error_note": "max over domains of max|mixed - FP64| / max|FP64| per conservative "
+                              "variable over the interior, after %d steps of both (the FP64 "
+                              "batch matches the oracle to <= 1e-10 in the parity tests)"
+                              % bm["steps_compared"],
+            }
     value = whole_job_rate(cells, world, a.steps, step_ms)
     e2e_value = whole_job_rate(cells, world, e2e_steps, e2e_ms)
 
