@@ -67,26 +67,55 @@ struct WallRoot {
 __host__ __device__ __forceinline__ double md_vap(double T) { return 1.0 - 1.91 * sqrt(1.0 - T); }
 __host__ __device__ __forceinline__ double md_liq(double T) { return 1.0 + 2.06 * sqrt(1.0 - T); }
 
-// wall_x_equilibrium_root_fct(md_x(2), [md_x(1), x], ...), :2151-2212
-__host__ __device__ double wall_root_f(const WallRoot& c, double x, const DimConst& k) {
-  const double dmddx_half = (-c.md1 + x) / (c.dxn);
-  const double md_av = 0.5 * (c.md1 + x);
-  const double gx = (x - c.md2) / (2.0 * c.dxn);        // dmddx, interior type
-  double gy;                                            // dmddx, :2433-2461
+// wall_x_equilibrium_root_fct(md_x(2), [md_x(1), x], ...), :2151-2212,
+// with its per-column constants computed once (WallRootFn) and the algebra
+// reduced: with s = sqrt(1 - Tav), md_liq - md_vap = 3.97 s and the surface
+// tension is a constant times s^3 (:2238-2270, dim2d_state_eq_module.f:
+// 56-227), so the energy-derivative term is
+//   6 cos(angle) (md_av - md_liq)(md_av - md_vap) st / (md_liq - md_vap)^3
+//   = C (md_av - md_liq)(md_av - md_vap),   C = 6 cos(angle) 2 sqrt(2)/(3 sqrt(We)) 9.6917.../3.97^3
+// and an evaluation is one square root and a dozen multiply-adds instead of
+// four divisions and three square roots (the solve runs one thread per
+// wall column, so its instruction chain is the kernel's duration).  The
+// value differs from the reference's evaluation order by rounding only.
+struct WallRootFn {
+  double md1, md2;
+  double a1;    // 1/(We delta_x): dmddx_half / We
+  double a2;    // 1/(2 delta_x): interior gradient normal to the wall
+  double gy2;   // square of the tangential density gradient (get_dmd_dx type of the column)
+  double base;  // Ed/md - |v|^2/2 + 3 md, the temperature without its gradient term
+  double cw;    // 1/(2 We md)
+  double c38;   // 3/(8 cv_r)
+  double tq;    // temperature jump of the heat flux, :2295-2315
+  double C;
+};
+
+__host__ __device__ __forceinline__ WallRootFn wall_root_fn(const WallRoot& c, const DimConst& k) {
+  WallRootFn w;
+  double gy;
   if (c.gt == WG_L0) gy = (c.my1 - c.md1) / c.dyt;
   else if (c.gt == WG_R0) gy = (c.md1 - c.my0) / c.dyt;
   else gy = (c.my1 - c.my0) / (2.0 * c.dyt);
-  const double g2 = gx * gx + gy * gy;
-  const double T1 = 3.0 / (8.0 * k.cv_r) *
-                    (c.Ed / c.md1 - 0.5 * (c.vx * c.vx + c.vy * c.vy) -
-                     0.5 / k.we * g2 / c.md1 + 3.0 * c.md1);           // :2382-2407
-  const double Tav = T1 + 0.5 * c.dxn * k.re * k.pr * 3.0 / (8.0 * k.cv_r) * c.q;  // :2295-2315
-  const double mv = md_vap(Tav), ml = md_liq(Tav);
+  w.md1 = c.md1;
+  w.md2 = c.md2;
+  w.a1 = 1.0 / (k.we * c.dxn);
+  w.a2 = 0.5 / c.dxn;
+  w.gy2 = gy * gy;
+  w.base = c.Ed / c.md1 - 0.5 * (c.vx * c.vx + c.vy * c.vy) + 3.0 * c.md1;
+  w.cw = 0.5 / (k.we * c.md1);
+  w.c38 = 3.0 / (8.0 * k.cv_r);
+  w.tq = 0.5 * c.dxn * k.re * k.pr * w.c38 * c.q;
+  w.C = 6.0 * c.cosang * (2.0 * sqrt(2.0) / (3.0 * sqrt(k.we)) * 9.691686257306483) /
+        (3.97 * 3.97 * 3.97);
+  return w;
+}
+
+__host__ __device__ __forceinline__ double wall_root_f(const WallRootFn& w, double x) {
+  const double gx = (x - w.md2) * w.a2;
+  const double Tav = w.c38 * (w.base - w.cw * (gx * gx + w.gy2)) + w.tq;
   const double s = sqrt(1.0 - Tav);
-  const double st = 2.0 * sqrt(2.0) / (3.0 * sqrt(k.we)) * (9.691686257306483 * (s * s * s));
-  const double d = ml - mv;
-  const double dE = 6.0 * (md_av - ml) * (md_av - mv) / (d * d * d) * st * c.cosang;  // :2238-2270
-  return 1.0 / k.we * dmddx_half + dE;
+  const double md_av = 0.5 * (w.md1 + x);
+  return w.a1 * (x - w.md1) + w.C * (md_av - (1.0 + 2.06 * s)) * (md_av - (1.0 - 1.91 * s));
 }
 
 __host__ __device__ __forceinline__ bool same_sign(double a, double b) {
@@ -97,24 +126,43 @@ __host__ __device__ __forceinline__ bool validated(double a, double b) { return 
 // :1846-1941 then ridders_method_module.f:112-216.  Returns the root;
 // *status gets 1 (no bracket), 2 (not bracketed), 3 (no convergence) or
 // 4 (bracketing error).
+//
+// The sequence of trial points and tests is the reference's; only the order
+// of evaluation is changed for latency (one thread per wall column, so the
+// chain of dependent root-function calls is the kernel's duration): the
+// bracket ends, the guess and the first scan pair are evaluated together,
+// before the tests that use them, and Ridders' method starts from the
+// function values of its bracket ends already computed (the reference
+// evaluates them again; the function is deterministic, so the values and
+// the result are the same).
 __host__ __device__ double wall_root(const WallRoot& c, double T_guess, double md_guess,
                                      const DimConst& k, unsigned int* status) {
+  const WallRootFn w = wall_root_fn(c, k);
   double xl = md_vap(T_guess), xh = md_liq(T_guess);
-  double fl = wall_root_f(c, xl, k), fh = wall_root_f(c, xh, k);
+  const double dmd_l = md_guess / 100.0, dmd_r = (3.0 - md_guess) / 100.0;
+  const double a1 = md_guess - 1 * dmd_l, b1 = md_guess + 1 * dmd_r;
+  double fl = wall_root_f(w, xl), fh = wall_root_f(w, xh);
+  const double fmd = wall_root_f(w, md_guess);
+  const double fa1 = wall_root_f(w, a1), fb1 = wall_root_f(w, b1);
   if (same_sign(fl, fh)) {
-    const double dmd_l = md_guess / 100.0, dmd_r = (3.0 - md_guess) / 100.0;
-    const double fmd = wall_root_f(c, md_guess, k);
     bool found = false;
     for (int j = 1; j <= 99 && !found; j++) {
       const double a = md_guess - j * dmd_l, b = md_guess + j * dmd_r;
-      const double fa = wall_root_f(c, a, k), fb = wall_root_f(c, b, k);
+      const double fa = j == 1 ? fa1 : wall_root_f(w, a);
       if (!same_sign(fa, fmd)) {
         xl = a;
         xh = md_guess;
+        fl = fa;
+        fh = fmd;
         found = true;
-      } else if (!same_sign(fb, fmd)) {
+        break;
+      }
+      const double fb = j == 1 ? fb1 : wall_root_f(w, b);
+      if (!same_sign(fb, fmd)) {
         xl = md_guess;
         xh = b;
+        fl = fmd;
+        fh = fb;
         found = true;
       }
     }
@@ -123,24 +171,22 @@ __host__ __device__ double wall_root(const WallRoot& c, double T_guess, double m
       return NAN;
     }
   }
-  // Ridders' method
+  // Ridders' method, from the bracket [xl, xh] and its values fl, fh
   const double xacc = 1e-12;
   const double UNUSED = (double)(-1.11e30f);
-  fl = wall_root_f(c, xl, k);
-  fh = wall_root_f(c, xh, k);
   double x = UNUSED;
   if ((fl > 0.0 && fh < 0.0) || (fl < 0.0 && fh > 0.0)) {
     const double x1 = xl;
     (void)x1;
     for (int j = 1; j <= 60; j++) {
       const double xm = 0.5 * (xl + xh);
-      const double fm = wall_root_f(c, xm, k);
+      const double fm = wall_root_f(w, xm);
       const double s = sqrt(fm * fm - fl * fh);
       if (validated(s, 0.0)) return x;
       const double xnew = xm + (xm - xl) * (copysign(1.0, fl - fh) * fm / s);
       if (fabs(xnew - x) <= xacc) return x;
       x = xnew;
-      const double fnew = wall_root_f(c, x, k);
+      const double fnew = wall_root_f(w, x);
       if (validated(fnew, 0.0)) return x;
       if (!validated(copysign(fm, fnew), fm)) {
         xl = xm;
