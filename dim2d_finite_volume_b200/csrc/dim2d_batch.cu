@@ -6,7 +6,9 @@
 // borrows their device buffers.  Members are grouped by boundary kind:
 //   G_PERIODIC  periodic_xy            strip kernel writes the ghost images
 //   G_OPEN      hedstrom_xy            ghost cells fused into the launch
-//   G_WALL      wall_S_reflection      strip kernel + node boundary pass
+//   G_WALL      wall_S_reflection,     strip kernel + node boundary pass; the
+//               wall_S_open,           open sections' ghost cells fused into
+//               half_wall_S_open       the launch
 //   G_MIRROR    reflection_xy          strip kernel + node boundary pass
 // and by precision (groups 4..7: the same kinds, DIM2D_MIXED fields).
 // One RK stage of a group is one batched launch over all its domains (plus
@@ -108,6 +110,7 @@ cudaError_t group_stage(dim2d_batch* b, int g, const std::vector<int>& idx, int 
       d.xmap0 = h->xmap0;
       d.periodic = h->periodic;
       d.wall_s = h->south_wall;
+      d.open = h->open_mask;
       NodeBcDomain& q = Q.d[j];
       q.utmp = h->A;
       q.u = out;
@@ -120,6 +123,9 @@ cudaError_t group_stage(dim2d_batch* b, int g, const std::vector<int>& idx, int 
       q.ymap0 = h->ymap0;
       q.south_wall = h->south_wall;
       q.corners_y = h->corners_y;
+      q.open_w = h->open_w;
+      q.open_e = h->open_e;
+      q.open_n = h->open_n;
       q.status = h->status;
     }
     cudaError_t e = launch_strip_batch(P, kind_of(g), shape, is_mixed(g), s);
@@ -255,10 +261,6 @@ int dim2d_batch_add(dim2d_batch* b, dim2d_handle* h, double dt) {
     return set_error(DIM2D_ERR_UNSUPPORTED,
                      "batch_add: batch members must share the physical constants");
   if (h->f.pitch % 2 != 0) return set_error(DIM2D_ERR_UNSUPPORTED, "batch_add: odd pitch");
-  if (h->open_mask && !h->open_all)
-    return set_error(DIM2D_ERR_UNSUPPORTED,
-                     "batch_add: wall_S_open / half_wall_S_open fields step on their own "
-                     "(no batched kernel for open sections beside a wall)");
   // the batch's work follows what was queued on the field's stream,
   // including an asynchronous download of the field
   cudaError_t e = cudaSuccess;

@@ -133,6 +133,7 @@ struct BatchDomain {
   double* uout;
   double dx, dy, rdx, rdy, dt, xmap0;
   int periodic, wall_s;
+  int open;                // OPEN_* mask of the time-integrated ghost sections
   int ghost0, strip0, sx;  // first ghost CTA, first strip CTA, strips per row
 };
 
@@ -142,11 +143,13 @@ struct BatchStageArgs {
   int stage;
   double b;
   int ndom;
-  int ghost_ctas;  // total ghost CTAs (open kind), placed before all strips
+  int ghost_ctas;  // total ghost CTAs (open and wall kinds), placed before all strips
   BatchDomain d[BATCH_MAX];
 };
 
-// boundary kinds of a batched stage launch
+// boundary kinds of a batched stage launch; BK_WALL launches also integrate
+// the open sections of wall_S_open / half_wall_S_open members (their
+// ghost CTAs first; wall_S_reflection members have none)
 enum BatchKind : int { BK_PLAIN = 0, BK_WALL = 1, BK_OPEN = 2 };
 
 // one stage of every domain in P (shape as launch_strip_stage; mixed: the
@@ -160,6 +163,7 @@ struct NodeBcDomain {
   Field f;
   double dx, dy, rdx, rdy, xmap0, ymap0;
   int south_wall, corners_y;
+  int open_w, open_e, open_n;
   unsigned int* status;
   int cta0;
 };

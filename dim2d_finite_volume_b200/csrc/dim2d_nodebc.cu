@@ -429,7 +429,9 @@ __host__ __device__ __forceinline__ NodeBcArgs batch_node_args(const NodeBcBatch
   a.ymap0 = d.ymap0;
   a.south_wall = d.south_wall;
   a.corners_y = d.corners_y;
-  a.open_w = a.open_e = a.open_n = 0;
+  a.open_w = d.open_w;
+  a.open_e = d.open_e;
+  a.open_n = d.open_n;
   a.status = d.status;
   a.wall = P.wall;
   a.k = P.k;

@@ -570,7 +570,7 @@ __device__ __forceinline__ StageArgs batch_stage_args(const BatchStageArgs& P, i
   a.wall_w = a.wall_e = a.wall_n = 0;
   a.wall_s = d.wall_s;
   a.variant = 0;
-  a.open = 0;
+  a.open = d.open;
   a.mixed = 0;
   a.t = 0.0;
   a.xmap0 = d.xmap0;
@@ -594,16 +594,16 @@ __device__ __forceinline__ int batch_domain(const BatchStageArgs& P, int b) {
 }
 
 // One RK stage of every domain of a batch (one boundary kind): the ghost
-// CTAs of all domains first (open kind), then every domain's strip CTAs.
+// CTAs of all domains first (open and wall kinds: each domain's open
+// sections), then every domain's strip CTAs.
 template <int H, int WPC, int MINB, int KIND, bool MIX>
 __global__ void __launch_bounds__(32 * WPC, MINB)
     k_strip_batch(const __grid_constant__ BatchStageArgs P) {
   int b = blockIdx.x;
-  if (KIND == K_OPEN) {
+  if (KIND == K_OPEN || KIND == K_WALL_OPEN) {
     if (b < P.ghost_ctas) {
       const int i = batch_domain<true>(P, b);
-      StageArgs a = batch_stage_args(P, i);
-      a.open = OPEN_ALL;
+      const StageArgs a = batch_stage_args(P, i);
       open_ghost_cell(a, (b - P.d[i].ghost0) * (32 * WPC) + threadIdx.x, 1);
       return;
     }
@@ -611,7 +611,8 @@ __global__ void __launch_bounds__(32 * WPC, MINB)
   }
   const int i = batch_domain<false>(P, b);
   const StageArgs a = batch_stage_args(P, i);
-  strip_cta<H, WPC, 1, KIND == K_WALL, MIX>(a, b - P.d[i].strip0, P.d[i].sx);
+  strip_cta<H, WPC, 1, KIND == K_WALL || KIND == K_WALL_OPEN, MIX>(a, b - P.d[i].strip0,
+                                                                     P.d[i].sx);
 }
 
 #undef ST
@@ -651,7 +652,7 @@ cudaError_t launch_strip_shape(const StageArgs& a, int mode, cudaStream_t s) {
 
 template <int H, int WPC, int MINB, bool MIX>
 const void* strip_batch_fn(int kind) {
-  return kind == BK_WALL   ? (const void*)k_strip_batch<H, WPC, MINB, K_WALL, MIX>
+  return kind == BK_WALL   ? (const void*)k_strip_batch<H, WPC, MINB, K_WALL_OPEN, MIX>
          : kind == BK_OPEN ? (const void*)k_strip_batch<H, WPC, MINB, K_OPEN, MIX>
                            : (const void*)k_strip_batch<H, WPC, MINB, K_PLAIN, MIX>;
 }
@@ -670,7 +671,8 @@ cudaError_t launch_strip_batch_shape(BatchStageArgs& P, int kind, bool mixed, cu
     const int sy = (d.f.ny - 2 * BC + H * WPC - 1) / (H * WPC);
     d.ghost0 = (int)ghost;
     d.strip0 = (int)strips;
-    if (kind == BK_OPEN) ghost += (open_ghost_count(d.f, OPEN_ALL) + 32 * WPC - 1) / (32 * WPC);
+    if (kind == BK_OPEN || kind == BK_WALL)
+      ghost += (open_ghost_count(d.f, d.open) + 32 * WPC - 1) / (32 * WPC);
     strips += (long long)d.sx * sy;
   }
   if (ghost + strips > 0x7fffffffLL) return cudaErrorInvalidValue;

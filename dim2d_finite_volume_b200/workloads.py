@@ -116,13 +116,14 @@ def served_params():
 
 
 def served_requests(seed, count, rate=50.0, n_range=(64, 1024), steps_range=(500, 20000),
-                    mixed_fraction=0.5):
+                    mixed_fraction=0.5, kinds=SERVED_KINDS):
     """Served stream: Poisson arrivals at `rate` per second; grid size n
     (square) log-uniform in n_range, step count uniform in steps_range,
     T0 in U[0.9, 0.99], wall or open boundaries, one bubble of radius in
     U[0.05, 0.2] (open fields: Mach in U[0, 0.1]), FP64 or mixed precision
     (a `mixed_fraction` share, drawn from a separate seeded stream).  Each
     request carries its arrival time (s) from the start of the stream.
+    `kinds`: the boundary presets drawn from (uniformly).
     The bubbles have the equilibrium interface width at T0 for We =
     SERVED_WE (ic.interface_length), as the reference's bubble initial
     conditions do; solve them with served_params()."""
@@ -137,7 +138,7 @@ def served_requests(seed, count, rate=50.0, n_range=(64, 1024), steps_range=(500
         steps = int(rng.integers(steps_range[0], steps_range[1] + 1))
         T0 = float(rng.uniform(0.90, 0.99))
         r = float(rng.uniform(0.05, 0.2))
-        bc = SERVED_KINDS[int(rng.integers(0, len(SERVED_KINDS)))]
+        bc = kinds[int(rng.integers(0, len(kinds)))]
         mach = float(rng.uniform(0.0, 0.1)) if bc == "hedstrom_xy" else 0.0
         d = domain(n, T0=T0, bubbles=[(0.0, 0.0, r)], mach=mach, bc=bc,
                    li=ic.interface_length(T0, SERVED_WE), we=SERVED_WE)

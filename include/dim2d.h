@@ -250,8 +250,8 @@ DIM2D_API int dim2d_step_noalloc(const dim2d_params *p, int nx, int ny, const in
  * Members are fields created with dim2d_create and uploaded, on the
  * batch's device, sharing one dim2d_params (FP64 and DIM2D_MIXED fields
  * form separate groups); the batch borrows their
- * buffers and advances their state and time.  wall_S_open and
- * half_wall_S_open fields cannot join a batch (DIM2D_ERR_UNSUPPORTED).
+ * buffers and advances their state and time (wall_S_open and
+ * half_wall_S_open fields join the wall_S_reflection chain).
  * While a field is a member,
  * dim2d_step on it is refused; dim2d_download/dim2d_time_dev of a member
  * are ordered after the batch's queued steps.  dim2d_destroy of a member

@@ -28,7 +28,8 @@ def B():
 # (preset, interior n, ny, seed)
 MIX = [("periodic_xy", 64, 48, 1), ("hedstrom_xy", 70, 52, 2), ("wall_S_reflection", 56, 40, 3),
        ("reflection_xy", 48, 64, 4), ("periodic_xy", 33, 97, 5), ("hedstrom_xy", 100, 40, 6),
-       ("wall_S_reflection", 90, 72, 7)]
+       ("wall_S_reflection", 90, 72, 7), ("half_wall_S_open", 66, 50, 8),
+       ("wall_S_open", 45, 61, 9)]
 
 
 def _case(preset, n, ny, seed):
@@ -92,7 +93,7 @@ def test_mixed_batch_matches_fields_alone(oracle, F, B, graphs):
 
 
 def test_batch_matches_oracle(oracle, F, B):
-    picks = [MIX[0], MIX[1], MIX[2]]
+    picks = [MIX[0], MIX[1], MIX[2], MIX[7], MIX[8]]
     cases = [(p,) + _prepared(oracle, F, p, n, ny, s) for p, n, ny, s in picks]
     fields = []
     with B.Batch() as bt:
@@ -211,7 +212,7 @@ def test_fp64_and_mixed_members_in_one_batch(oracle, F, B):
     """Mixed-precision members form their own groups; each member's result
     equals the field alone: FP64 to 1e-12, mixed to 1e-6 (the FP32 face
     pass of the batched kernel against the single-field kernel)."""
-    picks = [MIX[0], MIX[1], MIX[2], MIX[3]]
+    picks = [MIX[0], MIX[1], MIX[2], MIX[3], MIX[7]]
     cases = [(p,) + _prepared(oracle, F, p, n, ny, s) for p, n, ny, s in picks]
     fields, precs = [], []
     with B.Batch() as bt:

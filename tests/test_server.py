@@ -26,10 +26,11 @@ def S():
     return server
 
 
-def _requests(count, seed, n_range=(36, 110)):
+def _requests(count, seed, n_range=(36, 110), kinds=None):
     from dim2d_finite_volume_b200 import workloads
     return workloads.served_requests(seed, count, rate=200.0, n_range=n_range,
-                                     steps_range=(20, 90))
+                                     steps_range=(20, 90),
+                                     kinds=kinds or workloads.SERVED_KINDS)
 
 
 def _params():
@@ -74,6 +75,24 @@ def test_results_same_alone_and_in_the_mix(F, S):
         assert np.all(_err(got, ref, r["bc"]) <= _bar(r)), (i, r["nx"], r["bc"], r["precision"])
         assert abs(t - t_ref) <= 1e-12 * t_ref
         assert run["latencies"][i] > 0
+
+
+def test_open_wall_presets_same_alone_and_in_the_mix(F, S):
+    """Requests of the reference's default preset (half_wall_S_open) and of
+    wall_S_open share the wall chain of the batched launches with
+    wall_S_reflection requests."""
+    reqs = _requests(8, seed=33, kinds=("half_wall_S_open", "wall_S_open", "wall_S_reflection",
+                                        "hedstrom_xy"))
+    assert {r["bc"] for r in reqs} >= {"half_wall_S_open", "wall_S_open"}
+    with S.Server(params=_params(), chunk_steps=16) as srv:
+        run = S.serve(srv, reqs, keep_results=True)
+    assert run["stats"]["completed"] == len(reqs)
+    assert run["failed"] == []
+    for i, r in enumerate(reqs):
+        got, t = run["results"][i]
+        ref, t_ref = _alone(F, r)
+        assert np.isfinite(got[:, 2:-2, 2:-2]).all()
+        assert np.all(_err(got, ref, r["bc"]) <= _bar(r)), (i, r["nx"], r["bc"], r["precision"])
 
 
 def test_admission_by_memory_budget(F, S):
