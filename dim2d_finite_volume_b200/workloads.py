@@ -79,11 +79,27 @@ def plain_1024(seed, n=1024, bc="hedstrom_xy"):
 BATCH_KINDS = ("wall_S_reflection", "periodic_xy", "hedstrom_xy")
 
 
+# Weber number of the batched configuration (one constant set: the domains
+# share batched launches); equilibrium interface widths 0.08-0.26 over T0 in
+# [0.9, 0.99], so that every domain runs the configuration's 2000 steps
+BATCH_WE = 2000.0
+
+
+def batch_params():
+    """dim2d_params of the batched configuration (We = BATCH_WE)."""
+    from .field import default_params
+    p = default_params()
+    p.we = BATCH_WE
+    return p
+
+
 def batched_domains(seed, count=64, sizes=tuple(range(128, 513, 64))):
     """Batched FP64: `count` independent domains, n uniform in
     {128, 192, ..., 512} (square), T0 in U[0.90, 0.99], bubble radius in
     U[0.05, 0.2], boundary kind uniform over wall / periodic / open, flow
-    Mach in U[0, 0.1] for open domains (wall and periodic domains at rest)."""
+    Mach in U[0, 0.1] for open domains (wall and periodic domains at rest).
+    The bubbles have the equilibrium interface width at T0 for We =
+    BATCH_WE (ic.interface_length); solve them with batch_params()."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
@@ -93,7 +109,7 @@ def batched_domains(seed, count=64, sizes=tuple(range(128, 513, 64))):
         mach = float(rng.uniform(0.0, 0.1))
         bc = BATCH_KINDS[int(rng.integers(0, len(BATCH_KINDS)))]
         d = domain(n, T0=T0, bubbles=[(0.0, 0.0, r)], mach=mach if bc == "hedstrom_xy" else 0.0,
-                   bc=bc)
+                   bc=bc, li=ic.interface_length(T0, BATCH_WE), we=BATCH_WE)
         d["radius"] = r
         out.append(d)
     return out
