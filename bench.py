@@ -351,6 +351,7 @@ def run_batched_mixed(a, stream, barrier, F, Bm, torch, flush, doms, fields64, t
     FP64 batch, then advanced to the FP64 fields' step count and compared
     with them (normwise over each interior, max over domains; the FP64
     batch matches the oracle to 1e-10 in the parity tests)."""
+    from dim2d_finite_volume_b200 import workloads
     fields = []
     for d in doms:
         fld = F.Field(d["nx"], d["ny"], bc=d["bc"], precision=F.MIXED,
