@@ -384,12 +384,16 @@ def run_batched_mixed(a, stream, barrier, F, Bm, torch, flush, doms, fields64, t
     err = np.zeros(4)
     abs_err = np.zeros(4)
     scale = np.zeros(4)
-    for fm, f64 in zip(fields, fields64):
+    by_kind = {}
+    for fm, f64, d in zip(fields, fields64, doms):
         qm, qd = fm.download(), f64.download()
+        kind = by_kind.setdefault(d["bc"], np.zeros(4))
         for v in range(4):
             b_ = qd[v, 2:-2, 2:-2]
             d_ = float(np.abs(qm[v, 2:-2, 2:-2] - b_).max())
-            err[v] = max(err[v], d_ / float(np.abs(b_).max()))
+            r_ = d_ / float(np.abs(b_).max())
+            err[v] = max(err[v], r_)
+            kind[v] = max(kind[v], r_)
             abs_err[v] = max(abs_err[v], d_)
             scale[v] = max(scale[v], float(np.abs(b_).max()))
         fm.close()
@@ -397,6 +401,7 @@ def run_batched_mixed(a, stream, barrier, F, Bm, torch, flush, doms, fields64, t
             "steps_compared": total_steps, "rel_err_vs_fp64": [float(e) for e in err],
             "abs_err_vs_fp64": [float(e) for e in abs_err],
             "max_abs_fp64": [float(e) for e in scale], "clocks": mclocks,
+            "rel_err_by_kind": {k: [float(e) for e in v] for k, v in by_kind.items()},
             "block_ms_per_step": [round(min(per_block), 4), round(max(per_block), 4)]}
 
 
@@ -651,6 +656,7 @@ def main():
                 "rel_err_vs_fp64": bm["rel_err_vs_fp64"],
                 "abs_err_vs_fp64": bm["abs_err_vs_fp64"],
                 "max_abs_fp64": bm["max_abs_fp64"],
+                "rel_err_by_kind": bm["rel_err_by_kind"],
                 "error_bar": 1e-5,
                 "error_note": "per conservative variable (rho, rho u, rho v, rho E): max over "
                               "domains of max|mixed - FP64| / max|FP64| over each interior, after "
