@@ -486,7 +486,10 @@ int dim2d_autotune(dim2d_handle* h, int* chosen, double* times_ms) {
                   : h->open_all ? 1
                   : h->open_mask ? 4 + h->open_w
                   : h->south_wall ? 2 : 3;
-  const long long key = ((long long)h->f.nx << 32) ^ ((long long)h->f.ny << 4) ^ cls;
+  // size, boundary class (bits 0-2) and precision (bit 3): the FP64 and the
+  // mixed-precision kernels of one size may prefer different shapes
+  const long long key = ((long long)h->f.nx << 32) ^ ((long long)h->f.ny << 4) ^
+                        ((long long)(h->precision == DIM2D_MIXED) << 3) ^ cls;
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     auto it = g_tune.find(key);
