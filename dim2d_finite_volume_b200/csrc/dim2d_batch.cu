@@ -111,6 +111,7 @@ cudaError_t group_stage(dim2d_batch* b, int g, const std::vector<int>& idx, int 
       d.periodic = h->periodic;
       d.wall_s = h->south_wall;
       d.open = h->open_mask;
+      d.node_sides = st >= 2 && has_node_pass(g) ? h->node_sides : 0;
       NodeBcDomain& q = Q.d[j];
       q.utmp = h->A;
       q.u = out;

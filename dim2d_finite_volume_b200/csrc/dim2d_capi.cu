@@ -253,10 +253,12 @@ int dim2d::create_field(const dim2d_params* p, int nx, int ny, const int bc_choi
   h->south_wall = south_wall;
   h->corners_y = corners_y;
   if (open) h->open_mask = OPEN_ALL;
+  if (mirrors) h->node_sides = NODE_W | NODE_E | NODE_S | NODE_N;
   if (open_wall) {
     h->open_n = h->open_e = 1;
     h->open_w = open_w;
     h->open_mask = OPEN_N | OPEN_E | OPEN_NE | (open_w ? OPEN_W | OPEN_NW : 0);
+    h->node_sides = NODE_S | (open_w ? 0 : NODE_W);
   }
   h->wall = make_wall(*p);
   std::memcpy(h->bc_choice, bc_choice, sizeof h->bc_choice);

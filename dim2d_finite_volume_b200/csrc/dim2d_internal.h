@@ -23,6 +23,8 @@ struct dim2d_handle {
   // presets wall_S_open / half_wall_S_open
   int open_mask = 0;
   int open_w = 0, open_e = 0, open_n = 0;
+  // dim2d::NODE_* sides whose ghost cells the node pass writes (mirrors, wall)
+  int node_sides = 0;
   dim2d::WallConst wall{};
   unsigned int* status = nullptr;  // wall root status word (device)
   double xmap0 = 0, ymap0 = 0;     // x_map(1), y_map(1)

@@ -62,9 +62,16 @@ struct StageArgs {
   int mixed;                           // DIM2D_MIXED: FP32 face pass (strip kernels)
   double t;                            // field time (constant over the stages)
   double xmap0, ymap0;                 // x_map(1), y_map(1): x_map(i) = xmap0 + (i-1) dx
+  int node_sides;                      // NODE_* sides whose ghost cells the node pass just
+                                       // before this launch writes; non-zero: the launch is
+                                       // a programmatic dependent of that pass and the
+                                       // warps that read those ghosts wait for it
   WallConst wall;
   DimConst k;
 };
+
+// sides of StageArgs::node_sides
+enum NodeSide : int { NODE_W = 1, NODE_E = 2, NODE_S = 4, NODE_N = 8 };
 
 // Node boundary pass of a field whose sides are mirrors (reflection_x/_y),
 // open (nothing to do) or, on the south side, the wall operator.
@@ -134,6 +141,7 @@ struct BatchDomain {
   double dx, dy, rdx, rdy, dt, xmap0;
   int periodic, wall_s;
   int open;                // OPEN_* mask of the time-integrated ghost sections
+  int node_sides;          // as StageArgs::node_sides
   int ghost0, strip0, sx;  // first ghost CTA, first strip CTA, strips per row
 };
 

@@ -409,7 +409,14 @@ __host__ __device__ void node_bc_cell(const NodeBcArgs& a, int m) {
 }
 
 namespace {
+// the stage launch that follows may start at once (programmatic dependent
+// launch); its warps that read this pass's ghost cells wait for its end
+__device__ __forceinline__ void allow_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 __global__ void __launch_bounds__(128) k_node_bc(NodeBcArgs a) {
+  allow_dependents();
   node_bc_cell(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
@@ -441,6 +448,7 @@ __host__ __device__ __forceinline__ NodeBcArgs batch_node_args(const NodeBcBatch
 // node boundary pass of every domain of a batch: CTAs [cta0_i, cta0_i+1)
 // belong to domain i
 __global__ void __launch_bounds__(128) k_node_bc_batch(const __grid_constant__ NodeBcBatchArgs P) {
+  allow_dependents();
   const int b = blockIdx.x;
   int lo = 0, hi = P.ndom - 1;
   while (lo < hi) {

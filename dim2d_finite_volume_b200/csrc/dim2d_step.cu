@@ -36,6 +36,9 @@ StageArgs make_stage_args(const dim2d_handle* h, const double* uin, double* uout
   a.t = h->t;
   a.xmap0 = h->xmap0;
   a.ymap0 = h->ymap0;
+  // stages 2 and 3 follow the node pass of the stage before (stage()): they
+  // may start while it runs, only the warps that read its ghosts wait
+  a.node_sides = st >= 2 ? h->node_sides : 0;
   a.wall = h->wall;
   a.k = h->k;
   return a;

@@ -82,6 +82,23 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// A stage launched as a programmatic dependent of the node pass before it
+// (StageArgs::node_sides != 0) starts while that pass runs: a warp whose
+// rows or columns reach a side the pass writes waits for the pass (and its
+// memory) before its first read; the other warps read only cells the
+// previous stage wrote, complete before the pass began.
+__device__ __forceinline__ void wait_for_node_pass() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+}
+// 1 if the warp's reads -- columns c0-2 .. c0+31, rows y0-2 .. y1+2 (the
+// last one a prefetch past the strip), clamped to the field -- reach a
+// ghost cell of the sides in `sides`
+__device__ __forceinline__ bool reads_node_ghosts(int sides, const Field& f, int c0, int y0,
+                                                  int y1) {
+  return ((sides & NODE_W) && c0 - 2 < BC) || ((sides & NODE_E) && c0 + 31 >= f.nx - BC) ||
+         ((sides & NODE_S) && y0 - 2 < BC) || ((sides & NODE_N) && y1 + 2 >= f.ny - BC);
+}
+
 // state row `row` into the ring row at offset o (which includes the lane),
 // asynchronously: lane p < 17 copies the 16-byte pairs of columns
 // c0-2+2p, c0-1+2p of the 4 planes.  Addresses are clamped to the field's
@@ -413,6 +430,8 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
                                : NS * ST_ROW + NUV * UV_ROW + NQ * Q_ROW) + lane;
   int un0 = unb, un1 = unb + UN_ROW;
 
+  if (a.node_sides && reads_node_ghosts(a.node_sides, f, c0, y0, y1)) wait_for_node_pass();
+
   // prologue: state rows y0-2, y0-1, y0, y0+1 (s3, s2, s0, s1), all four
   // copies in flight together; node quantities of rows y0-1 (um, q1) and
   // y0 (u0, q0); bottom face of row y0; then row y0+2 (into s2) and u^n of
@@ -543,6 +562,7 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost
   int b = blockIdx.x;
   if (KIND == K_OPEN || KIND == K_WALL_OPEN) {
     if (b < ghost_ctas) {
+      if (a.node_sides) wait_for_node_pass();  // ghost frames reach the wall rows
       open_ghost_cell(a, b * (32 * WPC) + threadIdx.x, MODE);
       return;
     }
@@ -571,6 +591,7 @@ __device__ __forceinline__ StageArgs batch_stage_args(const BatchStageArgs& P, i
   a.wall_s = d.wall_s;
   a.variant = 0;
   a.open = d.open;
+  a.node_sides = d.node_sides;
   a.mixed = 0;
   a.t = 0.0;
   a.xmap0 = d.xmap0;
@@ -604,6 +625,7 @@ __global__ void __launch_bounds__(32 * WPC, MINB)
     if (b < P.ghost_ctas) {
       const int i = batch_domain<true>(P, b);
       const StageArgs a = batch_stage_args(P, i);
+      if (a.node_sides) wait_for_node_pass();
       open_ghost_cell(a, (b - P.d[i].ghost0) * (32 * WPC) + threadIdx.x, 1);
       return;
     }
@@ -620,6 +642,24 @@ __global__ void __launch_bounds__(32 * WPC, MINB)
 #undef NQ_
 #undef FQ
 #undef KQ
+
+// launch; with `after_node_pass`, as a programmatic dependent of the node
+// pass launched just before on `s` (it may start while the pass runs)
+inline cudaError_t launch_after_node_pass(const void* fn, unsigned blocks, unsigned threads,
+                                          size_t smem, cudaStream_t s, bool after_node_pass,
+                                          void** args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = after_node_pass ? 1 : 0;
+  return cudaLaunchKernelExC(&cfg, fn, args);
+}
 
 template <int H, int WPC, int MINB, int MODE, bool MIX>
 const void* strip_fn(int kind) {
@@ -647,7 +687,7 @@ cudaError_t launch_strip_shape(const StageArgs& a, int mode, cudaStream_t s) {
   const unsigned blocks = (unsigned)ghost_ctas + (unsigned)sx * (unsigned)sy;
   StageArgs aa = a;
   void* args[] = {&aa, &ghost_ctas, &sx};
-  return cudaLaunchKernel(fn, dim3(blocks), dim3(32 * WPC), args, smem, s);
+  return launch_after_node_pass(fn, blocks, 32 * WPC, smem, s, a.node_sides != 0, args);
 }
 
 template <int H, int WPC, int MINB, bool MIX>
@@ -677,8 +717,10 @@ cudaError_t launch_strip_batch_shape(BatchStageArgs& P, int kind, bool mixed, cu
   }
   if (ghost + strips > 0x7fffffffLL) return cudaErrorInvalidValue;
   P.ghost_ctas = (int)ghost;
+  bool pdl = false;
+  for (int i = 0; i < P.ndom; i++) pdl = pdl || P.d[i].node_sides != 0;
   void* args[] = {&P};
-  return cudaLaunchKernel(fn, dim3((unsigned)(ghost + strips)), dim3(32 * WPC), args, smem, s);
+  return launch_after_node_pass(fn, (unsigned)(ghost + strips), 32 * WPC, smem, s, pdl, args);
 }
 
 }  // namespace
