@@ -155,6 +155,17 @@ def library():
                                   + [_dp, _dp]),
         "dim2d_last_error": (ctypes.c_char_p, []),
         "dim2d_version": (ctypes.c_char_p, []),
+        "dim2d_time_dev_masked": (ctypes.c_int, [ctypes.POINTER(Params), ctypes.c_int,
+                                                 ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_double, ctypes.c_double,
+                                                 ctypes.POINTER(ctypes.c_int),
+                                                 ctypes.POINTER(ctypes.c_int), ctypes.c_void_p,
+                                                 ctypes.c_void_p]),
+        "dim2d_rk_stage_masked": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_double, ctypes.POINTER(ctypes.c_int),
+                                                 ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -188,6 +199,30 @@ def pinned_empty(shape):
     arr = np.frombuffer(buf, dtype=np.float64, count=n).reshape(shape)
     weakref.finalize(arr, library().dim2d_host_free, p)
     return arr
+
+
+# ---- buffer-layer grids (bf_layer): masked interior operators on device
+# arrays the caller owns (addresses as integers, e.g. torch.Tensor.data_ptr())
+NO_PT, INTERIOR_PT, BC_INTERIOR_PT, BC_PT = 0, 1, 2, 3  # parameters_bf_layer.f:41-44
+
+
+def time_dev_masked(params, nx, ny, nodes_ptr, grdpts_id_ptr, dx, dy, x_borders, y_borders,
+                    time_dev_ptr, stream=0):
+    """td_operators%compute_time_dev_nopt's interior part on the device:
+    time_dev at the interior_pt points inside the (1-based) borders."""
+    arr = ctypes.c_int * 2
+    _check(library().dim2d_time_dev_masked(ctypes.byref(params), nx, ny, nodes_ptr,
+                                           grdpts_id_ptr, dx, dy, arr(*x_borders),
+                                           arr(*y_borders), time_dev_ptr, stream))
+
+
+def rk_stage_masked(stage, nx, ny, nodes_ptr, nodes_tmp_ptr, time_dev_ptr, grdpts_id_ptr, dt,
+                    x_borders, y_borders, stream=0):
+    """compute_1st/2nd/3rd_step_nopt on the device, in place."""
+    arr = ctypes.c_int * 2
+    _check(library().dim2d_rk_stage_masked(stage, nx, ny, nodes_ptr, nodes_tmp_ptr,
+                                           time_dev_ptr, grdpts_id_ptr, dt, arr(*x_borders),
+                                           arr(*y_borders), stream))
 
 
 def _ptr(a):

@@ -242,6 +242,36 @@ DIM2D_API int dim2d_step_noalloc(const dim2d_params *p, int nx, int ny, const in
                                  const double *x_map, const double *y_map, double dt,
                                  int nsteps, void *stream);
 
+/* ---- Masked operators of buffer-layer grids.  A buffer layer carries its
+ * own nodes(nx,ny,4) and grdpts_id(nx,ny) map: no_pt 0, interior_pt 1,
+ * bc_interior_pt 2, bc_pt 3 (parameters_bf_layer.f:41-44).  These two calls
+ * do the area-sized work of stepping one on the device; the layer's
+ * boundary sections (bc_pt / bc_interior_pt points) remain the host-driven
+ * layer code's.  All arrays are device pointers owned by the caller, in the
+ * reference's layout (pitch nx); borders are 1-based inclusive, host arrays;
+ * `stream` is a cudaStream_t (NULL = legacy default stream); the calls
+ * return without synchronising and allocate nothing.
+ *
+ * Time derivative at the interior_pt points inside the borders (and at
+ * least bc_size points from the grid's edges), written into time_dev;
+ * every other point of time_dev is left as it is.  Every face of an
+ * interior_pt point must lie between interior_pt / bc_interior_pt points,
+ * as the reference's layers are built.
+ * Replaces: the interior part of td_operators%compute_time_dev_nopt
+ * (td_operators_class.f:293-417, fluxes pmodel_eq_class.f:1215-1360). */
+DIM2D_API int dim2d_time_dev_masked(const dim2d_params *p, int nx, int ny, const double *nodes,
+                                    const int *grdpts_id, double dx, double dy,
+                                    const int x_borders[2], const int y_borders[2],
+                                    double *time_dev, void *stream);
+/* RK3-TVD stage `stage` (1, 2, 3) in place on nodes, nodes_tmp = u^n:
+ * stage 1 over every point that is not no_pt (nodes_tmp receives u^n),
+ * stages 2 and 3 over those inside the borders.
+ * Replaces: compute_1st/2nd/3rd_step_nopt (rk3tvd_steps_module.f:130-614). */
+DIM2D_API int dim2d_rk_stage_masked(int stage, int nx, int ny, double *nodes, double *nodes_tmp,
+                                    const double *time_dev, const int *grdpts_id, double dt,
+                                    const int x_borders[2], const int y_borders[2],
+                                    void *stream);
+
 /* ---- Batches: no counterpart in the reference (one field per process
  * there).  A batch advances many fields together: one launch per RK stage
  * per boundary kind covers all its fields, and a step is a captured CUDA

@@ -93,6 +93,15 @@ double orc_speed_of_sound(const double q[4]);
 void orc_compute_time_dev(const orc_cfg *c, double t, const double *nodes,
                           const double *x_map, const double *y_map,
                           double *time_dev);
+/* masked ("_nopt") interior operators of buffer-layer grids
+ * (dim2d_oracle_masked.c): grdpts_id(nx,ny) with no_pt 0, interior_pt 1,
+ * bc_interior_pt 2, bc_pt 3; borders 1-based inclusive */
+void orc_compute_time_dev_masked(int nx, int ny, const double *nodes, const int *grdpts_id,
+                                 double dx, double dy, const int xb[2], const int yb[2],
+                                 double *time_dev);
+void orc_rk_stage_masked(int stage, int nx, int ny, double *nodes, double *nodes_tmp,
+                         const double *time_dev, const int *grdpts_id, double dt,
+                         const int xb[2], const int yb[2]);
 /* field_abstract_class.f:447-463 -> bc dispatcher */
 void orc_apply_bc_on_nodes(const orc_cfg *c, double t, const double *x_map,
                            const double *y_map, const double *nodes_tmp,

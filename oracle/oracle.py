@@ -82,6 +82,13 @@ def lib():
         L.orc_get_params.argtypes = [ctypes.POINTER(Params)]
         L.orc_set_threads.argtypes = [ctypes.c_int]
         L.orc_debug_real.restype = ctypes.c_double
+        _ip = ctypes.POINTER(ctypes.c_int)
+        L.orc_compute_time_dev_masked.restype = None
+        L.orc_compute_time_dev_masked.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _ip,
+                                                  ctypes.c_double, ctypes.c_double, _ip, _ip, _dp]
+        L.orc_rk_stage_masked.restype = None
+        L.orc_rk_stage_masked.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp,
+                                          _ip, ctypes.c_double, _ip, _ip]
         _lib = L
     return _lib
 
@@ -147,6 +154,30 @@ def integrate(cfg, nodes, x_map, y_map, t, dt, nsteps):
     if rc != 0:
         raise RuntimeError("oracle integrate failed: %d" % rc)
     return tt.value
+
+
+def _iptr(a):
+    assert a.dtype == np.int32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def compute_time_dev_masked(nodes, grdpts_id, dx, dy, x_borders, y_borders, time_dev):
+    """Masked interior time derivative of a buffer-layer grid, written into
+    time_dev at its interior_pt points (nodes [4][ny][nx], grdpts_id
+    [ny][nx] int32, borders 1-based inclusive)."""
+    ny, nx = grdpts_id.shape
+    xb = np.array(x_borders, dtype=np.int32)
+    yb = np.array(y_borders, dtype=np.int32)
+    lib().orc_compute_time_dev_masked(nx, ny, ptr(nodes), _iptr(grdpts_id), dx, dy, _iptr(xb),
+                                      _iptr(yb), ptr(time_dev))
+
+
+def rk_stage_masked(stage, nodes, nodes_tmp, time_dev, grdpts_id, dt, x_borders, y_borders):
+    ny, nx = grdpts_id.shape
+    xb = np.array(x_borders, dtype=np.int32)
+    yb = np.array(y_borders, dtype=np.int32)
+    lib().orc_rk_stage_masked(stage, nx, ny, ptr(nodes), ptr(nodes_tmp), ptr(time_dev),
+                              _iptr(grdpts_id), dt, _iptr(xb), _iptr(yb))
 
 
 def sd_operator(set_id, op, nodes, i, j, dx, dy):
