@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--mixed-steps", type=int, default=10000,
                     help="steps of the mixed-precision configuration (0: skip it)")
     ap.add_argument("--mixed-n", type=int, default=2048)
+    ap.add_argument("--buffer-layer", type=int, default=1,
+                    help="also time the masked buffer-layer operators (0: skip)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="precision of the plain workload")
     ap.add_argument("--served", type=int, default=32,
@@ -510,6 +512,87 @@ def run_mixed(a, stream, F, torch):
     }
 
 
+def run_buffer_layer(a, stream, F, torch, flush, peak):
+    """The masked (buffer-layer) operators on a 2048 x 256 edge band: a
+    RK3 step = 3 x (dim2d_time_dev_masked + dim2d_rk_stage_masked), on the
+    caller's device arrays (boundary points keep a zero time derivative).
+    Each step and each launch is bracketed by CUDA events on the launching
+    stream, L2 flushed before each.  Algorithmic bytes per layer point:
+    time derivative 32 (nodes) + 4 (grdpts_id) + 32 (time_dev) = 68;
+    stage 32 (nodes in) + 32 (time_dev) + 32 (nodes_tmp) + 32 (nodes out)
+    + 4 = 132; step 3 x (68 + 132) = 600."""
+    from dim2d_finite_volume_b200 import workloads
+    d = workloads.buffer_layer(a.seed + 5)
+    nx, ny, dt = d["nx"], d["ny"], d["dt"]
+    xb, yb = d["x_borders"], d["y_borders"]
+    g = d["grdpts_id"]
+    points = int((g != 0).sum())
+    u = torch.from_numpy(d["nodes"]).cuda()
+    tmp = torch.empty_like(u)
+    td = torch.zeros_like(u)
+    gid = torch.from_numpy(g).cuda()
+    p = F.default_params()
+    s = stream.cuda_stream
+
+    def td_call():
+        F.time_dev_masked(p, nx, ny, u.data_ptr(), gid.data_ptr(), d["dx"], d["dy"], xb, yb,
+                          td.data_ptr(), s)
+
+    def st_call(st):
+        F.rk_stage_masked(st, nx, ny, u.data_ptr(), tmp.data_ptr(), td.data_ptr(),
+                          gid.data_ptr(), dt, xb, yb, s)
+
+    def step():
+        for st in (1, 2, 3):
+            td_call()
+            st_call(st)
+
+    steps = max(5, a.steps)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        # at least W steps and ~0.3 s of work, so the clocks have ramped up
+        t0, n = time.perf_counter(), 0
+        while n < max(3, a.warmup) or time.perf_counter() - t0 < 0.3:
+            step()
+            n += 1
+            if n % 50 == 0:
+                torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        for e in ev:
+            flush.zero_()
+            e[0].record(stream)
+            step()
+            e[1].record(stream)
+        torch.cuda.synchronize()
+        step_ms = float(np.median([e[0].elapsed_time(e[1]) for e in ev]))
+        launch_ms = {}
+        for name, call in (("time_dev_masked", td_call), ("rk_stage_masked", lambda: st_call(2))):
+            for e in ev:
+                flush.zero_()
+                e[0].record(stream)
+                call()
+                e[1].record(stream)
+            torch.cuda.synchronize()
+            launch_ms[name] = float(np.median([e[0].elapsed_time(e[1]) for e in ev]))
+    finite = bool(torch.isfinite(u).all().item())
+    per_kernel = {}
+    for name, b in (("time_dev_masked", 68), ("rk_stage_masked", 132)):
+        gbs = b * points / (launch_ms[name] * 1e-3) / 1e9
+        per_kernel[name] = {"launch_ms": launch_ms[name], "algorithmic_bytes": b * points,
+                            "achieved_gbs": gbs, "frac": gbs / peak}
+    return {
+        "workload": "buffer layer: 2048 x 256 edge band of a 2048^2 domain (%d x %d grid, "
+                    "%d layer points), bubble crossing it in a Mach 0.1 flow" % (nx, ny, points),
+        "value": points / (step_ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": step_ms,
+        "steps": steps, "launches_per_step": 6, "finite": finite,
+        "roofline": {"bound": "hbm", "bytes_per_point_step": 600,
+                     "achieved_gbs": 600 * points / (step_ms * 1e-3) / 1e9,
+                     "frac": 600 * points / (step_ms * 1e-3) / 1e9 / peak,
+                     "per_kernel": per_kernel},
+        "timing": "median of CUDA-event brackets per step and per launch, L2 flushed before each",
+    }
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -611,6 +694,8 @@ def main():
         bres = run_batched(a, stream, barrier, F, torch, flush)
     served = run_served(a) if a.served > 0 else None
     mixed = run_mixed(a, stream, F, torch) if a.mixed_steps > 0 else None
+    layer = (run_buffer_layer(a, stream, F, torch, flush, measured_peaks()[0])
+             if a.buffer_layer else None)
 
     step_ms, e2e_ms = reduce_max([step_ms, e2e_ms], dist, "cuda")
     batched = None
@@ -724,6 +809,9 @@ def main():
                 line["served"] = served
             else:  # replicas: every rank served its own stream; report rank 0's
                 line["served"] = dict(served, note="rank 0 of %d replicas" % world)
+        if layer is not None:
+            line["buffer_layer"] = layer if dist is None else dict(
+                layer, note="rank 0 of %d replicas" % world)
         line["cpu_baseline"] = cpu_baseline(w, budget_s=a.cpu_budget)
         print(json.dumps(line), flush=True)
     if dist is not None:

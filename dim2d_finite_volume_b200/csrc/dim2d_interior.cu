@@ -36,7 +36,12 @@ constexpr int SM_FX = 4 * TY * (TX + 1);
 constexpr int SM_FY = 4 * (TY + 1) * TX;
 constexpr int SM_DOUBLES = SM_RAW + SM_PRIM + SM_FX + SM_FY;
 
-// mode: 0 = write L(u) (time derivative), 1 = RK stage update
+// mode: 0 = write L(u) (time derivative), 1 = RK stage update,
+// 2 = L(u) of a buffer-layer grid: tiles over [box_x0, box_x1] x
+// [box_y0, box_y1], written where the grdpts_id map is interior_pt.  A face
+// whose stencil reaches a no_pt node (whatever it holds) feeds only points
+// that are not interior_pt: every point within two of an interior_pt point is
+// a boundary point of the layer.
 template <int MODE, bool WALL>
 __global__ void __launch_bounds__(NT, 2) k_interior(StageArgs a) {
   extern __shared__ __align__(16) double sm[];
@@ -54,8 +59,8 @@ __global__ void __launch_bounds__(NT, 2) k_interior(StageArgs a) {
   double* sFy = sFx + SM_FX;
 
   const Field f = a.f;
-  const int x0 = BC + blockIdx.x * TX;
-  const int y0 = BC + blockIdx.y * TY;
+  const int x0 = (MODE == 2 ? a.box_x0 : BC) + blockIdx.x * TX;
+  const int y0 = (MODE == 2 ? a.box_y0 : BC) + blockIdx.y * TY;
   const int tid = threadIdx.x;
 
   // 1. halo tile of the input state (rows are contiguous in HBM)
@@ -201,6 +206,7 @@ __global__ void __launch_bounds__(NT, 2) k_interior(StageArgs a) {
   const int o = (ty + 2) * LX + tx + 2;
   const double uc[4] = {sR[o], sMx[o], sMy[o], sE[o]};
   const size_t go = (size_t)gy * f.pitch + gx;
+  if (MODE == 2 && (gx > a.box_x1 || gy > a.box_y1 || __ldg(a.mask + go) != 1)) return;
   // periodic images of this cell in the ghost layers
   int ix2 = -1, iy2 = -1;
   if (a.periodic) {
@@ -221,7 +227,7 @@ __global__ void __launch_bounds__(NT, 2) k_interior(StageArgs a) {
       if (v == 3) L += -uc[2] * k.gravity;
     }
     double out;
-    if (MODE == 0) {
+    if (MODE != 1) {
       out = L;
     } else if (a.stage == 1) {
       out = uc[v] + a.dt * L;
@@ -299,8 +305,9 @@ static cudaError_t set_smem_attr() {
   if (e != cudaSuccess) return e;
   if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
   const int bytes = (int)interior_smem_bytes();
-  const void* fns[4] = {(const void*)k_interior<0, false>, (const void*)k_interior<1, false>,
-                        (const void*)k_interior<0, true>, (const void*)k_interior<1, true>};
+  const void* fns[5] = {(const void*)k_interior<0, false>, (const void*)k_interior<1, false>,
+                        (const void*)k_interior<0, true>, (const void*)k_interior<1, true>,
+                        (const void*)k_interior<2, false>};
   for (const void* fn : fns) {
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
@@ -327,6 +334,14 @@ cudaError_t launch_interior_stage(const StageArgs& a, cudaStream_t s) {
 }
 
 cudaError_t launch_time_dev(const StageArgs& a, cudaStream_t s) { return launch_mode<0>(a, s); }
+
+cudaError_t launch_time_dev_masked(const StageArgs& a, cudaStream_t s) {
+  cudaError_t e = set_smem_attr();
+  if (e != cudaSuccess) return e;
+  dim3 grid((a.box_x1 - a.box_x0 + TX) / TX, (a.box_y1 - a.box_y0 + TY) / TY);
+  k_interior<2, false><<<grid, NT, interior_smem_bytes(), s>>>(a);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_fill(double* p, double v, size_t n, cudaStream_t s) {
   int blocks = (int)((n + 255) / 256);

@@ -66,6 +66,11 @@ struct StageArgs {
                                        // before this launch writes; non-zero: the launch is
                                        // a programmatic dependent of that pass and the
                                        // warps that read those ghosts wait for it
+  const int* __restrict__ mask;        // time derivative of a buffer-layer grid: its
+                                       // grdpts_id map, written only where it is
+                                       // interior_pt (1) inside [box_x0, box_x1] x
+                                       // [box_y0, box_y1] (0-based, >= BC from the edges)
+  int box_x0, box_x1, box_y0, box_y1;
   WallConst wall;
   DimConst k;
 };
@@ -120,6 +125,8 @@ inline bool stage_fuses_open(const StageArgs& a) { return a.open && stage_uses_s
 constexpr int NUM_VARIANTS = 6;
 // L(a.uin) of the interior cells into a.uout (stage fields ignored)
 cudaError_t launch_time_dev(const StageArgs& a, cudaStream_t s);
+// L(u) of a buffer-layer grid at its interior_pt points (StageArgs::mask)
+cudaError_t launch_time_dev_masked(const StageArgs& a, cudaStream_t s);
 // open (Hedstrom) ghost cells of the sections in a.open; mode 0 writes
 // L(u) into a.uout, mode 1 the RK stage update
 cudaError_t launch_open_ghosts(const StageArgs& a, int mode, cudaStream_t s);

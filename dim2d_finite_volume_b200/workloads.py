@@ -194,3 +194,56 @@ def mixed_2048(seed, n=2048, count=4):
                li=ic.interface_length(0.97, MIXED_WE), we=MIXED_WE)
     d["bubbles"] = bub
     return d
+
+
+# grdpts_id values of buffer-layer grids (parameters_bf_layer.f:41-44)
+NO_PT, INTERIOR_PT, BC_INTERIOR_PT, BC_PT = 0, 1, 2, 3
+
+
+def layer_map(nx, ny, rects):
+    """grdpts_id [ny][nx] int32 of a buffer layer: interior_pt over the
+    union of the rectangles (0-based inclusive (x0, x1, y0, y1)), one ring
+    of bc_interior_pt around it, one ring of bc_pt around that, no_pt
+    elsewhere -- the layout the reference's layers keep around their
+    interior points."""
+    inner = np.zeros((ny, nx), bool)
+    for x0, x1, y0, y1 in rects:
+        inner[y0:y1 + 1, x0:x1 + 1] = True
+
+    def grow(m):  # 8-neighbour dilation without wrap-around
+        p = np.pad(m, 1)
+        out = np.zeros_like(m)
+        for sy in range(3):
+            for sx in range(3):
+                out |= p[sy:sy + ny, sx:sx + nx]
+        return out
+
+    ring1 = grow(inner) & ~inner
+    ring2 = grow(inner | ring1) & ~(inner | ring1)
+    g = np.zeros((ny, nx), np.int32)
+    g[ring2] = BC_PT
+    g[ring1] = BC_INTERIOR_PT
+    g[inner] = INTERIOR_PT
+    return g
+
+
+def buffer_layer(seed, n=2048, width=256, T0=0.95, mach=0.1):
+    """An edge band of a n^2 domain as a buffer layer grid: n x width
+    interior points of the domain's y range [0.5 - width dx, 0.5] extended
+    north, both boundary rings inside the (n + 4) x (width + 4) grid, and a
+    seeded bubble crossing the band in a Mach-`mach` x-flow.  Returns
+    dict(nx, ny, x_map, y_map, dx, dy, nodes, grdpts_id, dt, x_borders,
+    y_borders) with the reference's 1-based borders."""
+    rng = np.random.default_rng(seed)
+    dx = 1.0 / (n - 1)
+    y0 = 0.5 - (width - 1) * dx
+    nx, ny, x_map, y_map = ic.grid(n, width, y_min=y0, y_max=0.5)
+    r = float(rng.uniform(0.05, 0.1))
+    xc = float(rng.uniform(-0.3, 0.3))
+    u0 = mach * liquid_sound_speed(T0) if mach else 0.0
+    q = np.ascontiguousarray(ic.bubbles(x_map, y_map, T0, [(xc, y0 + 0.5 * r, r)],
+                                        li=4.0 * dx, velocity=(u0, 0.0)))
+    g = layer_map(nx, ny, [(2, nx - 3, 2, ny - 3)])
+    return dict(nx=nx, ny=ny, x_map=x_map, y_map=y_map, dx=dx, dy=y_map[1] - y_map[0],
+                nodes=q, grdpts_id=g, dt=stable_dt(q, dx, dx), x_borders=(3, nx - 2),
+                y_borders=(3, ny - 2))

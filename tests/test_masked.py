@@ -12,28 +12,8 @@ their values.  Bars (FP64): <= 1e-12 normwise for the time derivative,
 import numpy as np
 import pytest
 
+from dim2d_finite_volume_b200.workloads import layer_map
 from tests.helpers import periodic_case
-
-
-def layer_map(nx, ny, rects):
-    """grdpts_id [ny][nx] int32 from interior rectangles (0-based,
-    inclusive (x0, x1, y0, y1)), with the two boundary rings around them."""
-    g = np.zeros((ny, nx), np.int32)
-    inner = np.zeros((ny, nx), bool)
-    for x0, x1, y0, y1 in rects:
-        inner[y0:y1 + 1, x0:x1 + 1] = True
-    def dilate(m):
-        out = m.copy()
-        for dy in (-1, 0, 1):
-            for dx in (-1, 0, 1):
-                out |= np.roll(np.roll(m, dy, 0), dx, 1)
-        return out
-    ring1 = dilate(inner) & ~inner
-    ring2 = dilate(inner | ring1) & ~(inner | ring1)
-    g[ring2] = 3
-    g[ring1] = 2
-    g[inner] = 1
-    return g
 
 
 def _case(n=44, ny=36, seed=3):
@@ -41,6 +21,13 @@ def _case(n=44, ny=36, seed=3):
     # an L-shaped interior at least bc_size + 2 points from the edges
     g = layer_map(nx, nyy, [(4, nx - 5, 4, nyy // 2), (4, nx // 2, nyy // 2, nyy - 5)])
     return nx, nyy, x_map, y_map, np.ascontiguousarray(q), g
+
+
+def test_layer_map_rings():
+    g = layer_map(12, 10, [(4, 7, 3, 6)])
+    assert (g == 1).sum() == 16 and (g == 2).sum() == 20 and (g == 3).sum() == 28
+    assert g[0].tolist() == [0] * 12           # nothing wraps around the grid
+    assert g[3, 2] == 3 and g[3, 3] == 2 and g[3, 4] == 1
 
 
 def test_oracle_masked_matches_full_grid_on_interior_points(oracle):
