@@ -42,8 +42,10 @@ constexpr int SM_DOUBLES = SM_RAW + SM_PRIM + SM_FX + SM_FY;
 // whose stencil reaches a no_pt node (whatever it holds) feeds only points
 // that are not interior_pt: every point within two of an interior_pt point is
 // a boundary point of the layer.
+// Four 256-thread CTAs per SM (64 registers, no spills; 4 x 47.8 KB of shared
+// memory): with three, the face pass left the FP64 pipe waiting on latency.
 template <int MODE, bool WALL>
-__global__ void __launch_bounds__(NT, 2) k_interior(StageArgs a) {
+__global__ void __launch_bounds__(NT, 4) k_interior(StageArgs a) {
   extern __shared__ __align__(16) double sm[];
   double* sR = sm;
   double* sMx = sR + LX * LY;
@@ -310,6 +312,10 @@ static cudaError_t set_smem_attr() {
                         (const void*)k_interior<2, false>};
   for (const void* fn : fns) {
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    // four resident CTAs need the largest shared-memory carveout
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
   }
   if (dev >= 0 && dev < 64) done[dev] = true;
