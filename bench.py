@@ -115,6 +115,22 @@ def profile_traffic():
     return None
 
 
+def fp64_figures(bc):
+    """FP64 operations per cell-update from the committed counts
+    (profiles/fp64_ops.json): the stage kernel's executed FP64 thread
+    instructions from ncu, and the oracle's FP64 flops (the reference's
+    serial algorithm) from the counting build of oracle/flopcount.cpp."""
+    p = os.path.join(ROOT, "profiles", "fp64_ops.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    key = "%s_rk3_step" % (bc if bc == "periodic_xy" else "hedstrom_xy")
+    return {"kernel_inst": d["kernel_fp64_inst_per_cell_update"],
+            "kernel_flops": d["kernel_fp64_flops_per_cell_update"],
+            "oracle_flops": d["oracle"][key]["flops"], "oracle_key": key,
+            "kernel_workload": d["workload"]}
+
+
 class ClockSampler:
     def __init__(self, index):
         self.index = index
@@ -800,6 +816,22 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
+        f64 = fp64_figures(a.bc) if a.precision == "fp64" else None
+        if f64 is not None:
+            # FP64 lanes: 148 SMs x 64 per clock; DFMA counts as one instruction
+            mhz = float((clocks or {}).get("sm_max_mhz") or 1965.0)
+            peak_inst = 148 * 64 * mhz * 1e6
+            ach_inst = value * f64["kernel_inst"]
+            line["fp64"] = {
+                "kernel_inst_per_cell_update": f64["kernel_inst"],
+                "kernel_flops_per_cell_update": f64["kernel_flops"],
+                "oracle_flops_per_cell_update": f64["oracle_flops"],
+                "achieved_tinst_per_s": ach_inst / 1e12,
+                "peak_tinst_per_s": peak_inst / 1e12, "frac": ach_inst / peak_inst,
+                "note": ("FP64-ALU utilisation: the value's cell-updates/s x the stage kernel's "
+                         "FP64 thread instructions per cell-update (ncu, %s) / (148 SMs x 64 FP64 "
+                         "lanes x %.0f MHz); oracle: %s" % (f64["kernel_workload"], mhz,
+                                                           f64["oracle_key"]))}
         if batched is not None:
             line["batched"] = batched
         if mixed is not None:
