@@ -296,9 +296,9 @@ def run_batched(a, stream, barrier, F, torch, flush):
         if d["bc"] not in ("periodic_xy", "hedstrom_xy"):
             fld.apply_bc_on_nodes()  # field%ini
         fields.append(fld)
-    # plain form first: each field its own launches (its step graph)
-    for fld in fields:
-        fld.variant = 2
+    # plain form first: each field its own launches (its step graph), each
+    # with the stage-kernel variant the per-field autotuner picks for it
+    plain_variants = [fld.autotune()[0] for fld in fields]
     for _ in range(3):
         for fld, d in zip(fields, doms):
             fld.integrate(d["dt"], 1)
@@ -335,6 +335,7 @@ def run_batched(a, stream, barrier, F, torch, flush):
            "we": workloads.BATCH_WE, "clocks": bclocks,
            "block_ms_per_step": [round(min(per_block), 4), round(max(per_block), 4)],
            "plain_ms": plain_ms, "plain_steps": steps, "launches": int(launches),
+           "plain_variants": {str(v): plain_variants.count(v) for v in sorted(set(plain_variants))},
            "domains": len(doms), "shapes": shapes,
            "kinds": {k: sum(1 for d in doms if d["bc"] == k) for k in workloads.BATCH_KINDS}}
     if a.batch_mixed:
@@ -766,6 +767,7 @@ def main():
             "kinds": bres["kinds"], "shapes": bres["shapes"],
             "gpu_launches": bres["launches"],
             "plain_per_field_value": pv,
+            "plain_variants": bres["plain_variants"],
             "vs_plain_per_field": bv / pv,
             "roofline": {"bound": "hbm", "achieved": bv * BYTES_PER_CELL_UPDATE / 1e9,
                          "peak": peak_b, "unit": "GB/s",
@@ -773,7 +775,9 @@ def main():
             "timing": "CUDA events around blocks of 100 batched steps (each step one replay "
                       "of the batch's step graph), no L2 flush: the batch's state is several "
                       "times larger than L2; plain: the same fields stepped one after another, "
-                      "each by its own step graph, L2 flushed between steps",
+                      "each by its own step graph with the stage-kernel variant its own "
+                      "autotuner picked (plain_variants: variant -> fields), L2 flushed "
+                      "between steps (outside the events)",
             "clocks": bres["clocks"], "block_ms_per_step": bres["block_ms_per_step"],
         }
         if "mixed" in bres:
