@@ -194,12 +194,41 @@ def band_sample(w, rows, bottom=False):
     return q, np.ascontiguousarray(w["y_map"][lo:hi])
 
 
-def cpu_baseline(w, budget_s=15.0, threads=None):
+PARITY_STEPS = 3
+
+
+def parity_vs_oracle(O, w, q_gpu):
+    """Error of the GPU field after PARITY_STEPS RK3 steps against the
+    oracle's on the same initial state (the oracle as the checker): per
+    conservative variable, max|a - b| / max|b| and the L2 relative error
+    over the interior cells."""
+    nx, ny = w["nx"], w["ny"]
+    q = np.ascontiguousarray(w["nodes"], dtype=np.float64).copy()
+    cfg = oracle_cfg(O, w["bc"], nx, ny)
+    if w["bc"] not in ("periodic_xy", "hedstrom_xy"):
+        O.apply_bc_on_nodes(cfg, 0.0, w["x_map"], w["y_map"], q.copy(), q)
+    t0 = time.perf_counter()
+    O.integrate(cfg, q, w["x_map"], w["y_map"], 0.0, w["dt"], PARITY_STEPS)
+    el = time.perf_counter() - t0
+    a, b = q_gpu[:, 2:ny - 2, 2:nx - 2], q[:, 2:ny - 2, 2:nx - 2]
+    linf = [float(np.abs(a[k] - b[k]).max() / np.abs(b[k]).max()) for k in range(4)]
+    l2 = [float(np.sqrt(((a[k] - b[k]) ** 2).sum() / (b[k] ** 2).sum())) for k in range(4)]
+    return {"steps": PARITY_STEPS, "max_rel": linf, "l2_rel": l2, "oracle_s": round(el, 2),
+            "note": "GPU field vs the oracle after %d RK3 steps of the whole %dx%d field from "
+                    "the same initial state; per conservative variable (rho, rho u, rho v, "
+                    "rho E), interior cells: max|a-b|/max|b| and sqrt(sum (a-b)^2 / sum b^2)"
+                    % (PARITY_STEPS, nx, ny)}
+
+
+def cpu_baseline(w, budget_s=15.0, threads=None, gpu_state=None):
     """Oracle (CPU restatement) on a bounded sample: full RK3 steps of a
-    row band of the same field, repeated until budget_s of host time."""
+    row band of the same field, repeated until budget_s of host time.
+    With gpu_state (the GPU field after PARITY_STEPS steps), also the
+    error of that state against the oracle's."""
     from oracle import oracle as O
     nth = threads or os.cpu_count() or 1
     O.set_threads(nth)
+    parity = parity_vs_oracle(O, w, gpu_state) if gpu_state is not None else None
     nx = w["nx"]
     q, y_map = band_sample(w, 64, bottom=w["bc"] in WALL_PRESETS)
     band = q.shape[1]
@@ -214,11 +243,14 @@ def cpu_baseline(w, budget_s=15.0, threads=None):
         el = time.perf_counter() - t0
         if el >= budget_s:
             break
-    return {"value": cells * steps / el, "unit": "cell-updates/s", "cores": nth, "kind": "port",
-            "sample": "%d RK3 steps of a %dx%d %s band (interior %dx%d) %s of "
-                      "the %d^2 field, %.1f s" % (steps, nx, band, w["bc"], nx - 4, band - 4,
-                                                  "at the S wall" if w["bc"] in WALL_PRESETS
-                                                  else "through the centre", nx - 4, el)}
+    out = {"value": cells * steps / el, "unit": "cell-updates/s", "cores": nth, "kind": "port",
+           "sample": "%d RK3 steps of a %dx%d %s band (interior %dx%d) %s of "
+                     "the %d^2 field, %.1f s" % (steps, nx, band, w["bc"], nx - 4, band - 4,
+                                                 "at the S wall" if w["bc"] in WALL_PRESETS
+                                                 else "through the centre", nx - 4, el)}
+    if parity is not None:
+        out["parity"] = parity
+    return out
 
 
 def run_reference(a, rank, world):
@@ -740,6 +772,13 @@ def main():
     e2e_ms = e0.elapsed_time(e1)
     clocks = sampler.stop()
     fld2.close()
+    # ---- the headline field after PARITY_STEPS steps from its initial
+    # state, for the error against the oracle stated on the line
+    fld.ini(w["nodes"], w["x_map"], w["y_map"])
+    if a.bc not in ("periodic_xy", "hedstrom_xy"):
+        fld.apply_bc_on_nodes()  # field%ini
+    fld.integrate(dt, PARITY_STEPS)
+    q_gpu = fld.download()
     fld.close()
     bres = None
     if a.batch_domains > 0:
@@ -888,7 +927,7 @@ def main():
         if layer is not None:
             line["buffer_layer"] = layer if dist is None else dict(
                 layer, note="rank 0 of %d replicas" % world)
-        line["cpu_baseline"] = cpu_baseline(w, budget_s=a.cpu_budget)
+        line["cpu_baseline"] = cpu_baseline(w, budget_s=a.cpu_budget, gpu_state=q_gpu)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
