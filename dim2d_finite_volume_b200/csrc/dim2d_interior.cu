@@ -342,6 +342,7 @@ cudaError_t launch_interior_stage(const StageArgs& a, cudaStream_t s) {
 cudaError_t launch_time_dev(const StageArgs& a, cudaStream_t s) { return launch_mode<0>(a, s); }
 
 cudaError_t launch_time_dev_masked(const StageArgs& a, cudaStream_t s) {
+  if (strip_layout_ok(a)) return launch_strip_masked(a, s);
   cudaError_t e = set_smem_attr();
   if (e != cudaSuccess) return e;
   dim3 grid((a.box_x1 - a.box_x0 + TX) / TX, (a.box_y1 - a.box_y0 + TY) / TY);

@@ -125,8 +125,11 @@ inline bool stage_fuses_open(const StageArgs& a) { return a.open && stage_uses_s
 constexpr int NUM_VARIANTS = 6;
 // L(a.uin) of the interior cells into a.uout (stage fields ignored)
 cudaError_t launch_time_dev(const StageArgs& a, cudaStream_t s);
-// L(u) of a buffer-layer grid at its interior_pt points (StageArgs::mask)
+// L(u) of a buffer-layer grid at its interior_pt points (StageArgs::mask):
+// the strip kernel where strip_layout_ok (even nx, 16-byte aligned nodes),
+// else the tile kernel
 cudaError_t launch_time_dev_masked(const StageArgs& a, cudaStream_t s);
+cudaError_t launch_strip_masked(const StageArgs& a, cudaStream_t s);
 // open (Hedstrom) ghost cells of the sections in a.open; mode 0 writes
 // L(u) into a.uout, mode 1 the RK stage update
 cudaError_t launch_open_ghosts(const StageArgs& a, int mode, cudaStream_t s);

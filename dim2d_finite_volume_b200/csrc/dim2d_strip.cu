@@ -401,9 +401,11 @@ template <int H, int WPC, int MODE, bool WALL, bool MIX>
 __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const Field f = a.f;
-  const int c0 = BC + (b % sx) * SW;
-  const int y0 = BC + ((b / sx) * WPC + warp) * H;
-  const int ylast = f.ny - BC - 1;
+  // MODE 2 (buffer-layer grid): strips over the border box, the first one
+  // starting at an even column so that the rows' 16-byte pairs stay aligned
+  const int c0 = (MODE == 2 ? (a.box_x0 & ~1) : BC) + (b % sx) * SW;
+  const int y0 = (MODE == 2 ? a.box_y0 : BC) + ((b / sx) * WPC + warp) * H;
+  const int ylast = MODE == 2 ? a.box_y1 : f.ny - BC - 1;
   if (y0 > ylast) return;  // the whole warp leaves; no CTA barrier is used
   const int y1 = min(y0 + H, ylast + 1);
   const int x = c0 + lane;
@@ -459,7 +461,8 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
   if (need_un) async_un(a, x, y0, un0);
   cp_async_commit();
 
-  const bool active = lane < SW && x <= f.nx - 1 - BC;
+  const bool active = lane < SW && x <= f.nx - 1 - BC &&
+                      (MODE != 2 || (x >= a.box_x0 && x <= a.box_x1));
   int ix2 = -1;
   if (a.periodic) {
     const int px = f.nx - 2 * BC;
@@ -503,11 +506,12 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
           if (v == 2) L += -uc[0] * k.gravity;
           if (v == 3) L += -uc[2] * k.gravity;
         }
-        if (MODE == 0) out[v] = L;
+        if (MODE != 1) out[v] = L;
         else if (a.stage == 1) out[v] = uc[v] + a.dt * L;
         else out[v] = a.b * g_ring[un0 + v * 32] + (1.0 - a.b) * (uc[v] + a.dt * L);
       }
-      if (active) {
+      // MODE 2 writes the interior_pt points of the layer map only
+      if (active && (MODE != 2 || __ldg(a.mask + go) == 1)) {
 #pragma unroll
         for (int v = 0; v < 4; v++) a.uout[go + v * f.plane] = out[v];
         if (MODE == 1 && a.periodic) {  // periodic_xy/bc_operators_class.f:156-199
@@ -737,6 +741,33 @@ cudaError_t launch_strip_batch(BatchStageArgs& P, int kind, int shape, bool mixe
     case 4: return launch_strip_batch_shape<16, 8, 2>(P, kind, mixed, s);
   }
   return cudaErrorInvalidValue;
+}
+
+template <int H, int WPC, int MINB>
+cudaError_t launch_strip_masked_shape(const StageArgs& a, cudaStream_t s) {
+  const size_t smem = (size_t)WPC * WARP_DOUBLES * sizeof(double);
+  const void* fn = (const void*)k_strip<H, WPC, MINB, 2, K_PLAIN, false>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int sx = (a.box_x1 - (a.box_x0 & ~1) + SW) / SW;
+  const int sy = (a.box_y1 - a.box_y0 + H * WPC) / (H * WPC);
+  int ghost_ctas = 0;
+  StageArgs aa = a;
+  void* args[] = {&aa, &ghost_ctas, &sx};
+  return launch_after_node_pass(fn, (unsigned)sx * (unsigned)sy, 32 * WPC, smem, s, false, args);
+}
+
+// L(u) of a buffer-layer grid at its interior_pt points (MODE 2) over the
+// border box [box_x0, box_x1] x [box_y0, box_y1] (box_x0, box_y0 >= BC:
+// every copied row and column lies inside the grid).  Strips of 16 rows (2
+// warps per CTA, 8 CTAs per SM) where they fill the GPU's 148 x 16 warp
+// slots, else of 8 rows (4 warps per CTA) for twice the warps: layers are
+// often thin bands.  Needs strip_layout_ok(a).
+cudaError_t launch_strip_masked(const StageArgs& a, cudaStream_t s) {
+  const long long sx = (a.box_x1 - (a.box_x0 & ~1) + SW) / SW;
+  const long long warps16 = sx * ((a.box_y1 - a.box_y0 + 16) / 16);
+  if (warps16 >= 148LL * 16) return launch_strip_masked_shape<16, 2, 8>(a, s);
+  return launch_strip_masked_shape<8, 4, 4>(a, s);
 }
 
 // shape id -> (rows per warp, warps per CTA, minimum resident CTAs per SM

@@ -64,15 +64,28 @@ def _gpu_time_dev(F, torch, params, q, g, dx, dy, xb, yb, fill):
     return td.cpu().numpy()
 
 
+BORDERS = {"full": lambda nx, ny: ((3, nx - 2), (3, ny - 2)),
+           "narrow": lambda nx, ny: ((9, nx - 8), (6, ny - 10)),
+           # first border column 8: the box starts at the odd column 7
+           "odd": lambda nx, ny: ((8, nx - 7), (5, ny - 9))}
+
+
+# even nx: the warp-strip kernel (rows copied as 16-byte pairs), 8-row strips
+# where 16-row ones would not fill the GPU (2048 x 600 takes 16-row strips);
+# odd nx: the tile kernel; 100 x 83 spans several strips and row blocks, the
+# last ones partial
 @pytest.mark.gpu
-@pytest.mark.parametrize("borders", ["full", "narrow"])
-def test_time_dev_masked_matches_oracle(oracle, borders):
+@pytest.mark.parametrize("n,ny,borders", [(44, 36, "full"), (44, 36, "narrow"), (44, 36, "odd"),
+                                          (43, 36, "full"), (43, 36, "odd"),
+                                          (100, 83, "odd"), (100, 83, "full"),
+                                          (2048, 600, "odd")])
+def test_time_dev_masked_matches_oracle(oracle, n, ny, borders):
     import torch
 
     from dim2d_finite_volume_b200 import field as F
-    nx, ny, x_map, y_map, q, g = _case()
+    nx, ny, x_map, y_map, q, g = _case(n, ny)
     dx, dy = x_map[1] - x_map[0], y_map[1] - y_map[0]
-    xb, yb = ((3, nx - 2), (3, ny - 2)) if borders == "full" else ((9, nx - 8), (6, ny - 10))
+    xb, yb = BORDERS[borders](nx, ny)
     fill = np.full_like(q, 7.0)
     ref = fill.copy()
     oracle.compute_time_dev_masked(q, g, dx, dy, xb, yb, ref)
@@ -88,14 +101,15 @@ def test_time_dev_masked_matches_oracle(oracle, borders):
 
 
 @pytest.mark.gpu
-def test_masked_rk3_step_matches_oracle(oracle):
+@pytest.mark.parametrize("n", [44, 43])
+def test_masked_rk3_step_matches_oracle(oracle, n):
     """A whole masked step: time derivative, stage, three times; the layer's
     boundary points take a fixed time derivative, as its boundary sections
     would supply."""
     import torch
 
     from dim2d_finite_volume_b200 import field as F
-    nx, ny, x_map, y_map, q, g = _case(seed=5)
+    nx, ny, x_map, y_map, q, g = _case(n, seed=5)
     dx, dy = x_map[1] - x_map[0], y_map[1] - y_map[0]
     xb, yb = (3, nx - 2), (3, ny - 2)
     dt = 2e-6
