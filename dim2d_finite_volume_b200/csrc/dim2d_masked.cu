@@ -7,8 +7,10 @@
 // (3) (parameters_bf_layer.f:41-44).  These kernels are the area-sized part
 // of stepping such a grid:
 //   * time derivative at the interior_pt points inside the borders
-//     (td_operators_class.f:293-417): the interior tile kernel (k_interior,
-//     dim2d_interior.cu) over the border box, in its masked mode -- primitives
+//     (td_operators_class.f:293-417): the warp-strip kernel (k_strip,
+//     dim2d_strip.cu) where nx is even and the nodes 16-byte aligned, else
+//     the interior tile kernel (k_interior, dim2d_interior.cu), over the
+//     border box, in their masked mode -- primitives
 //     once per node, each face flux once with the interior Mattsson operators
 //     and the DIM flux formulas (every face of an interior_pt point lies
 //     between interior_pt / bc_interior_pt points, where the reference
