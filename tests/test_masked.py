@@ -102,6 +102,40 @@ def test_time_dev_masked_matches_oracle(oracle, n, ny, borders):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("n", [44, 43])
+def test_time_dev_masked_with_gravity(oracle, n):
+    """The body force (pmodel_eq_class.f:1840-1918) in the masked time
+    derivative: strip kernel (even nx) and tile kernel (odd nx)."""
+    import torch
+
+    from dim2d_finite_volume_b200 import field as F
+    nx, ny, x_map, y_map, q, g = _case(n, 36, seed=7)
+    dx, dy = x_map[1] - x_map[0], y_map[1] - y_map[0]
+    xb, yb = BORDERS["odd"](nx, ny)
+    fill = np.full_like(q, 7.0)
+    ref = fill.copy()
+    p0 = oracle.get_params()
+    try:
+        oracle.set_params(gravity_ac=1, gravity=0.7)
+        oracle.compute_time_dev_masked(q, g, dx, dy, xb, yb, ref)
+    finally:
+        oracle.set_params(**{name: getattr(p0, name) for name, _ in p0._fields_})
+    got = _gpu_time_dev(F, torch, F.default_params(gravity_ac=1, gravity=0.7), q, g, dx, dy,
+                        xb, yb, fill)
+    m = np.zeros_like(g, bool)
+    m[yb[0] - 1:yb[1], xb[0] - 1:xb[1]] = True
+    m &= g == 1
+    for k in range(4):
+        den = np.abs(ref[k][m]).max()
+        assert np.abs(got[k][m] - ref[k][m]).max() <= 1e-12 * den, k
+    # the body force changes the momentum_y and energy derivatives
+    plain = fill.copy()
+    oracle.compute_time_dev_masked(q, g, dx, dy, xb, yb, plain)
+    assert np.abs(ref[2][m] - plain[2][m]).max() > 5e-4 * np.abs(plain[2][m]).max()
+    assert np.all(got[:, ~m] == 7.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [44, 43])
 def test_masked_rk3_step_matches_oracle(oracle, n):
     """A whole masked step: time derivative, stage, three times; the layer's
     boundary points take a fixed time derivative, as its boundary sections
