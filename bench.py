@@ -23,6 +23,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -73,8 +74,9 @@ def parse():
                     help="precision of the plain workload")
     ap.add_argument("--served", type=int, default=32,
                     help="requests of the served stream (0: skip it)")
-    ap.add_argument("--cpu-budget", type=float, default=15.0,
-                    help="seconds of host time for the cpu_baseline sample")
+    ap.add_argument("--cpu-budget", type=float, default=None,
+                    help="no effect (the CPU legs time --steps steps of their sample); "
+                         "accepted so that older profiling command lines still run")
     return ap.parse_args()
 
 
@@ -139,9 +141,8 @@ class ClockSampler:
 
     def start(self):
         try:
-            os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-            self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % os.getpid())
-            self.fh = open(self.path, "w")
+            fd, self.path = tempfile.mkstemp(prefix="dim2d_clocks_", suffix=".csv")
+            self.fh = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index),
                  "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
@@ -162,9 +163,13 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         self.fh.close()
+        try:
+            lines = open(self.path).read().splitlines()
+        finally:
+            os.unlink(self.path)
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -220,79 +225,124 @@ def parity_vs_oracle(O, w, q_gpu):
                     % (PARITY_STEPS, nx, ny)}
 
 
-def cpu_baseline(w, budget_s=15.0, threads=None, gpu_state=None):
-    """Oracle (CPU restatement) on a bounded sample: full RK3 steps of a
-    row band of the same field, repeated until budget_s of host time.
-    With gpu_state (the GPU field after PARITY_STEPS steps), also the
-    error of that state against the oracle's."""
+CPU_SAMPLE_ROWS = 256  # interior rows of the CPU legs' sample of the field
+
+
+def cpu_sample(w):
+    """The sample both CPU legs time: a band of CPU_SAMPLE_ROWS interior
+    rows of the field (through its centre, or at the S wall for the wall
+    presets), or the whole field when it is not larger than that."""
+    if w["ny"] - 4 <= CPU_SAMPLE_ROWS:
+        return np.ascontiguousarray(w["nodes"]).copy(), w["y_map"], "all %dx%d nodes" % (
+            w["nx"], w["ny"])
+    q, y_map = band_sample(w, CPU_SAMPLE_ROWS, bottom=w["bc"] in WALL_PRESETS)
+    return q, y_map, "a %dx%d band (interior %dx%d) %s" % (
+        w["nx"], q.shape[1], w["nx"] - 4, q.shape[1] - 4,
+        "at the S wall" if w["bc"] in WALL_PRESETS else "through the centre")
+
+
+def host_cpu():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def cpu_measure(w, steps, warmup, threads):
+    """The reference algorithm on the host cores: the oracle's timing build
+    (-O3 -march=native, the checker's results bit for bit) with `threads`
+    OpenMP threads advances the sample by `warmup` untimed RK3 steps, then
+    `steps` RK3 steps each timed on its own (steady clock).  value = sample
+    cell-updates / median step time; best = over the fastest step."""
     from oracle import oracle as O
-    nth = threads or os.cpu_count() or 1
+    O.set_threads(threads)
+    O.fast_lib()
+    q, y_map, what = cpu_sample(w)
+    cfg = oracle_cfg(O, w["bc"], w["nx"], q.shape[1])
+    if w["bc"] != "hedstrom_xy":  # field%ini: node boundary pass
+        O.lib().orc_clear_status()
+        O.apply_bc_on_nodes(cfg, 0.0, w["x_map"], y_map, q.copy(), q)
+    cells = (w["nx"] - 4) * (q.shape[1] - 4)
+    t = 0.0
+    for _ in range(warmup):
+        t = O.integrate(cfg, q, w["x_map"], y_map, t, w["dt"], 1, fast=True)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        t = O.integrate(cfg, q, w["x_map"], y_map, t, w["dt"], 1, fast=True)
+        times.append(time.perf_counter() - t0)
+    med, best = float(np.median(times)), float(min(times))
+    return {"value": cells / med, "best": cells / best, "median_ms": 1e3 * med,
+            "best_ms": 1e3 * best, "steps": steps, "warmup": warmup, "cells": cells,
+            "threads": threads, "sample": what, "finite": bool(np.isfinite(q).all())}
+
+
+def cpu_baseline(w, steps, warmup, gpu_state=None):
+    """The CPU baseline on the line: the same measurement as the reference
+    arm (cpu_measure on all host threads, same sample, steps and warm-up),
+    the serial rate beside it (1 thread, 3 steps), and with gpu_state (the
+    GPU field after PARITY_STEPS steps) the error of that state against the
+    oracle's."""
+    from oracle import oracle as O
+    nth = os.cpu_count() or 1
     O.set_threads(nth)
     parity = parity_vs_oracle(O, w, gpu_state) if gpu_state is not None else None
-    nx = w["nx"]
-    q, y_map = band_sample(w, 64, bottom=w["bc"] in WALL_PRESETS)
-    band = q.shape[1]
-    cfg = oracle_cfg(O, w["bc"], nx, band)
-    O.apply_bc_on_nodes(cfg, 0.0, w["x_map"], y_map, q.copy(), q)
-    cells = (nx - 4) * (band - 4)
-    steps, t0 = 0, time.perf_counter()
-    t = 0.0
-    while True:
-        t = O.integrate(cfg, q, w["x_map"], y_map, t, w["dt"], 1)
-        steps += 1
-        el = time.perf_counter() - t0
-        if el >= budget_s:
-            break
-    out = {"value": cells * steps / el, "unit": "cell-updates/s", "cores": nth, "kind": "port",
-           "sample": "%d RK3 steps of a %dx%d %s band (interior %dx%d) %s of "
-                     "the %d^2 field, %.1f s" % (steps, nx, band, w["bc"], nx - 4, band - 4,
-                                                 "at the S wall" if w["bc"] in WALL_PRESETS
-                                                 else "through the centre", nx - 4, el)}
+    m = cpu_measure(w, steps, warmup, nth)
+    serial = cpu_measure(w, 3, 1, 1)
+    out = {"value": m["value"], "unit": "cell-updates/s", "cores": nth, "kind": "port",
+           "host": host_cpu(), "nproc": os.cpu_count(),
+           "sample": "each step: one RK3 step of %s of the %d^2 field; %d warm-up steps, then "
+                     "%d steps timed one by one; value over the median step, best over the "
+                     "fastest" % (m["sample"], w["nx"] - 4, warmup, steps),
+           "best": m["best"], "median_ms": m["median_ms"], "best_ms": m["best_ms"],
+           "build": "oracle timing build: gcc -O3 -march=native -ffp-contract=off -fopenmp "
+                    "(bit-identical to the -O2 checker build)",
+           "serial": {"value": serial["value"], "best": serial["best"], "cores": 1,
+                      "steps": 3}}
     if parity is not None:
         out["parity"] = parity
     return out
 
 
+def bench_config(a, w, nx, ny, dt):
+    """The `config` of both arms' lines (identical by construction)."""
+    return {"workload": "plain FP64 DIM %d^2 (+2 ghosts) bubble, T0=0.95, Mach %.1f flow, RK3 "
+                        "step" % (a.n, 0.1 if a.bc == "hedstrom_xy" else 0.0),
+            "bc": a.bc, "nx": nx, "ny": ny, "dt": dt, "seed": a.seed,
+            "l2": "GPU arm: flushed between timed steps (2x L2 write, outside the events); "
+                  "CPU arm: host arrays, no flush"}
+
+
 def run_reference(a, rank, world):
+    """The reference arm: the reference's CPU algorithm (the oracle's timing
+    build, all host threads) on this arm's workload, config and metric;
+    rank 0 only."""
     if rank != 0:
         return
-    from oracle import oracle as O
     w = workload(a.n, a.seed, bc=a.bc)
     nth = a.threads or os.cpu_count() or 1
-    O.set_threads(nth)
-    nx = w["nx"]
-    if w["ny"] <= 260:  # small fields are timed whole
-        q, y_map = np.ascontiguousarray(w["nodes"]), w["y_map"]
-    else:
-        q, y_map = band_sample(w, 32, bottom=a.bc in WALL_PRESETS)
-    band = q.shape[1]
-    cfg = oracle_cfg(O, a.bc, nx, band)
-    if a.bc != "hedstrom_xy":  # field%ini: node boundary pass
-        O.lib().orc_clear_status()
-        O.apply_bc_on_nodes(cfg, 0.0, w["x_map"], y_map, q.copy(), q)
-    cells = (nx - 4) * (band - 4)
-    t = 0.0
-    for _ in range(a.warmup):
-        t = O.integrate(cfg, q, w["x_map"], y_map, t, w["dt"], 1)
-    t0 = time.perf_counter()
-    for _ in range(a.steps):
-        t = O.integrate(cfg, q, w["x_map"], y_map, t, w["dt"], 1)
-    el = time.perf_counter() - t0
-    v = cells * a.steps / el
+    m = cpu_measure(w, a.steps, a.warmup, nth)
     line = {
-        "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": world,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * el / a.steps,
+        "metric": "cell-updates/s", "value": m["value"], "unit": "cell-updates/s",
+        "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": m["median_ms"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "impl": "reference",
-        "config": {"workload": "plain FP64 DIM %d^2 field, RK3 step, %s" % (
-                       a.n, "whole field" if band == w["ny"] else "row-band sample"),
-                   "sample_rows": band - 4, "bc": a.bc},
-        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": nth, "kind": "port",
-                         "sample": "each step: one RK3 step of %s of the %d^2 field"
-                                   % ("all %dx%d nodes" % (nx, band) if band == w["ny"]
-                                      else "a %dx%d band" % (nx, band), a.n)},
-        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+        "config": bench_config(a, w, w["nx"], w["ny"], w["dt"]),
+        "cpu_baseline": {"value": m["value"], "unit": "cell-updates/s", "cores": nth,
+                         "kind": "port", "host": host_cpu(), "nproc": os.cpu_count(),
+                         "best": m["best"], "median_ms": m["median_ms"],
+                         "best_ms": m["best_ms"],
+                         "sample": "each step: one RK3 step of %s of the %d^2 field; value over "
+                                   "the median step" % (m["sample"], a.n)},
+        "e2e": {"value": m["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "note": "the reference is Fortran and cannot be built on this image (no Fortran "
+                "compiler, no netCDF-Fortran): this arm times the oracle, the C restatement of "
+                "its algorithm, in its -O3 -march=native timing build",
     }
     print(json.dumps(line), flush=True)
 
@@ -465,7 +515,9 @@ def run_served(a):
     reqs = workloads.served_requests(a.seed + 99, a.served, rate=50.0)
     with Sm.Server(params=workloads.served_params(), chunk_steps=500) as srv:
         run = Sm.serve(srv, reqs)
-    lat = np.array(run["latencies"])
+    lat_all = np.array(run["latencies"])
+    fin = run["finished"]
+    lat = lat_all[fin] if fin else lat_all[:0]
     return {
         "workload": "served stream: %d requests, Poisson arrivals at 50/s, n log-uniform in "
                     "[64,1024], steps uniform in [500,20000], T0 in [0.90,0.99], wall "
@@ -473,21 +525,27 @@ def run_served(a):
                     "one bubble per request with the equilibrium interface width at T0, "
                     "We = %g for the whole stream"
                     % (len(reqs), sum(r["precision"] for r in reqs), workloads.SERVED_WE),
-        "value": run["cell_updates"] / run["wall_s"], "unit": "cell-updates/s",
-        "wall_s": run["wall_s"], "cell_updates": int(run["cell_updates"]),
-        "latency_p50_s": float(np.percentile(lat, 50)),
-        "latency_p99_s": float(np.percentile(lat, 99)),
-        "latency_max_s": float(lat.max()),
+        "value": run["cell_updates_finished"] / run["wall_s"], "unit": "cell-updates/s",
+        "value_note": "cell-updates of the requests that finished with a finite state (failed "
+                      "and non-finite requests excluded) / wall time of the whole stream; "
+                      "latencies likewise over the finished requests",
+        "wall_s": run["wall_s"], "cell_updates": int(run["cell_updates_finished"]),
+        "finished_requests": len(fin),
+        "latency_p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+        "latency_p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
+        "latency_max_s": float(lat.max()) if len(lat) else None,
+        "all_requests": {"value": run["cell_updates"] / run["wall_s"],
+                         "cell_updates": int(run["cell_updates"]),
+                         "latency_p50_s": float(np.percentile(lat_all, 50)),
+                         "latency_p99_s": float(np.percentile(lat_all, 99)),
+                         "note": "every request counted, failed and non-finite ones included"},
         "requests": len(reqs), "arrival_span_s": float(reqs[-1]["arrival"]),
         "max_active": int(run["stats"]["max_active"]),
         "failed_requests": len(run["failed"]),
         "nonfinite_requests": len(run["nonfinite"]),
         "failed_note": "failed = the wall ghost-cell root was not found (where the reference "
-                       "stops); non-finite = the solve blew up.  Open (Hedstrom) requests on "
-                       "small grids run long in physical time and meet the reference's "
-                       "open-boundary instability (velocity in the outermost ghost layer "
-                       "growing ~20x per unit time whatever the time step; the oracle blows up "
-                       "on the same inputs); their latency and cell-updates are still counted",
+                       "stops); non-finite = the solve blew up.  Both are left out of value and "
+                       "of the latency percentiles (all_requests keeps them)",
         "timing": "host wall clock from the first arrival to the last completion (the "
                   "stream is replayed in real time); latency = submit to completion",
     }
@@ -872,13 +930,10 @@ def main():
             "vs_baseline": None,
             "dtype": "f64" if a.precision == "fp64" else "f32 face pass + f64 (mixed)",
             "data": "synthetic",
-            "config": {"workload": "plain FP64 DIM %d^2 (+2 ghosts) bubble, T0=0.95, "
-                                   "Mach %.1f flow, RK3 step" % (a.n, 0.1 if a.bc == "hedstrom_xy"
-                                                                 else 0.0), "bc": a.bc, "nx": nx, "ny": ny, "dt": dt,
-                       "l2": "flushed between timed steps (2x L2 write, outside the events)",
-                       "replicas_per_gpu": 1, "stage_kernel": STAGE_KERNELS[variant],
-                       "autotune_ms": (None if tune_ms is None
-                                       else [round(float(x), 5) for x in tune_ms])},
+            "config": bench_config(a, w, nx, ny, dt),
+            "stage_kernel": STAGE_KERNELS[variant],
+            "autotune_ms": None if tune_ms is None else [round(float(x), 5) for x in tune_ms],
+            "replicas_per_gpu": 1,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "kernel": STAGE_KERNELS[variant] + " (fused RK3 stage)",
@@ -927,7 +982,7 @@ def main():
         if layer is not None:
             line["buffer_layer"] = layer if dist is None else dict(
                 layer, note="rank 0 of %d replicas" % world)
-        line["cpu_baseline"] = cpu_baseline(w, budget_s=a.cpu_budget, gpu_state=q_gpu)
+        line["cpu_baseline"] = cpu_baseline(w, a.steps, a.warmup, gpu_state=q_gpu)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

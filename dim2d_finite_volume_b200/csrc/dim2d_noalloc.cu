@@ -19,9 +19,17 @@
 //     call's contents: each call clears the part it uses before stepping,
 //     and calls that overlap on the GPU (different streams, or host
 //     threads not ordered by the caller) race on it;
-//   * the first call on a device, with that device current, looks up the
-//     array's device address once (cudaGetSymbolAddress); make that first
-//     call before any stream capture.
+//   * the first call in a CUDA context, with that context current, looks
+//     up the array's device address (cudaGetSymbolAddress) and keeps it
+//     for that context; make that first call before any stream capture.
+//     The cache is keyed by the context's unique id, so a new context on
+//     the same device (after cudaDeviceReset, or one made current with
+//     cuCtxSetCurrent) gets its own lookup;
+//   * boundary configurations: periodic_xy and hedstrom_xy only (the ones
+//     without a node boundary pass: no wall status word is needed);
+//   * after a non-zero return the contents of `nodes` are undefined.
+#include <cuda.h>
+
 #include <cmath>
 #include <mutex>
 
@@ -33,32 +41,92 @@ namespace {
 
 constexpr size_t kMaxCells = DIM2D_NOALLOC_MAX_CELLS;
 constexpr size_t kScratchDoubles = 2 * 4 * kMaxCells;
-constexpr int kMaxDevices = 64;
+constexpr int kMaxContexts = 64;
 
 // Two stage copies of the field; only device code and the looked-up
 // address below may touch it (in host code the name is a host-side
 // stand-in, not a device address).
 __device__ __align__(256) double g_stage_scratch[kScratchDoubles];
 
+// Unique id of the current CUDA context, through the driver entry point
+// (no link-time dependency on libcuda): cuCtxGetCurrent + cuCtxGetId.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+// 0 and *id set when a context is current; 1 when none is; else an error
+int current_context_id(unsigned long long* id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+    fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(fn);
+  });
+  if (!get_current || !get_id)
+    return set_error(DIM2D_ERR_CUDA, "step_noalloc: driver entry points cuCtxGetCurrent / "
+                                     "cuCtxGetId not available");
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS)
+    return set_error(DIM2D_ERR_CUDA, "step_noalloc: cuCtxGetCurrent failed");
+  if (!ctx) return 1;
+  if (get_id(ctx, id) != CUDA_SUCCESS)
+    return set_error(DIM2D_ERR_CUDA, "step_noalloc: cuCtxGetId failed");
+  return 0;
+}
+
 std::mutex g_scratch_mu;
-double* g_scratch_addr[kMaxDevices] = {};
+struct ScratchEntry {
+  unsigned long long ctx_id;
+  double* addr;
+};
+ScratchEntry g_scratch[kMaxContexts] = {};
+int g_scratch_n = 0;
+
+int lookup_symbol(double** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_stage_scratch);
+  if (e != cudaSuccess || !p)
+    return cuda_error(e == cudaSuccess ? cudaErrorInvalidSymbol : e,
+                      "step_noalloc: cudaGetSymbolAddress");
+  *out = static_cast<double*>(p);
+  return DIM2D_OK;
+}
 
 int scratch_address(double** out) {
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return cuda_error(e, "step_noalloc: cudaGetDevice");
-  if (dev < 0 || dev >= kMaxDevices)
-    return set_error(DIM2D_ERR_ARG, "step_noalloc: device %d out of range", dev);
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_stage_scratch);
-    if (e != cudaSuccess || !p)
-      return cuda_error(e == cudaSuccess ? cudaErrorInvalidSymbol : e,
-                        "step_noalloc: cudaGetSymbolAddress");
-    g_scratch_addr[dev] = static_cast<double*>(p);
+  unsigned long long id = 0;
+  int rc = current_context_id(&id);
+  double* addr = nullptr;
+  if (rc == 1) {
+    // no context yet: the runtime's first call binds the current device's
+    // primary context, then that context is the key
+    rc = lookup_symbol(&addr);
+    if (rc) return rc;
+    rc = current_context_id(&id);
+    if (rc == 1) return set_error(DIM2D_ERR_CUDA, "step_noalloc: no current CUDA context");
   }
-  *out = g_scratch_addr[dev];
+  if (rc) return rc;
+  for (int i = 0; i < g_scratch_n; i++)
+    if (g_scratch[i].ctx_id == id) {
+      *out = g_scratch[i].addr;
+      return DIM2D_OK;
+    }
+  if (!addr) {
+    rc = lookup_symbol(&addr);
+    if (rc) return rc;
+  }
+  // a full table reuses a slot (the context that held it gets looked up
+  // again if it is still alive)
+  const int slot = g_scratch_n < kMaxContexts ? g_scratch_n++ : (int)(id % kMaxContexts);
+  g_scratch[slot] = ScratchEntry{id, addr};
+  *out = addr;
   return DIM2D_OK;
 }
 

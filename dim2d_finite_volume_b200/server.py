@@ -128,7 +128,9 @@ def serve(server, requests, keep_results=False):
     its arrival time, the loop polls in between.  Returns dict(latencies, results (index ->
     (nodes, time) if keep_results), failed (indices of requests whose wall
     root failed), nonfinite (other requests whose final state is not
-    finite), wall_s, cell_updates, stats)."""
+    finite), finished (the other requests: finite solves), wall_s,
+    cell_updates (all requests), cell_updates_finished (finished requests
+    only), stats)."""
     order = sorted(range(len(requests)), key=lambda i: requests[i]["arrival"])
     ids = {}
     out, lat, failed, nonfinite = {}, {}, [], []
@@ -159,8 +161,14 @@ def serve(server, requests, keep_results=False):
             if keep_results:
                 out[i] = (res[0], res[1])
     wall = time.perf_counter() - t0
-    cu = sum(r["nsteps"] * (r["nodes"].shape[1] - 4) * (r["nodes"].shape[2] - 4)
-             for r in requests)
+    def cells(r):
+        return r["nsteps"] * (r["nodes"].shape[1] - 4) * (r["nodes"].shape[2] - 4)
+
+    bad = set(failed) | set(nonfinite)
     return dict(latencies=[lat[i] for i in range(len(requests))], results=out,
                 failed=sorted(failed), nonfinite=sorted(nonfinite), wall_s=wall,
-                cell_updates=cu, stats=server.stats())
+                cell_updates=sum(cells(r) for r in requests),
+                finished=[i for i in range(len(requests)) if i not in bad],
+                cell_updates_finished=sum(cells(r) for i, r in enumerate(requests)
+                                          if i not in bad),
+                stats=server.stats())

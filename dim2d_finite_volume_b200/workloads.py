@@ -93,13 +93,9 @@ def batch_params():
     return p
 
 
-def batched_domains(seed, count=64, sizes=tuple(range(128, 513, 64))):
-    """Batched FP64: `count` independent domains, n uniform in
-    {128, 192, ..., 512} (square), T0 in U[0.90, 0.99], bubble radius in
-    U[0.05, 0.2], boundary kind uniform over wall / periodic / open, flow
-    Mach in U[0, 0.1] for open domains (wall and periodic domains at rest).
-    The bubbles have the equilibrium interface width at T0 for We =
-    BATCH_WE (ic.interface_length); solve them with batch_params()."""
+def batched_specs(seed, count=64, sizes=tuple(range(128, 513, 64))):
+    """The seeded draws of batched_domains without building the fields: one
+    dict(n, T0, radius, mach, bc) per domain, in order."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
@@ -108,11 +104,27 @@ def batched_domains(seed, count=64, sizes=tuple(range(128, 513, 64))):
         r = float(rng.uniform(0.05, 0.2))
         mach = float(rng.uniform(0.0, 0.1))
         bc = BATCH_KINDS[int(rng.integers(0, len(BATCH_KINDS)))]
-        d = domain(n, T0=T0, bubbles=[(0.0, 0.0, r)], mach=mach if bc == "hedstrom_xy" else 0.0,
-                   bc=bc, li=ic.interface_length(T0, BATCH_WE), we=BATCH_WE)
-        d["radius"] = r
-        out.append(d)
+        out.append(dict(n=n, T0=T0, radius=r, mach=mach if bc == "hedstrom_xy" else 0.0, bc=bc))
     return out
+
+
+def batched_domain(spec):
+    """The field of one batched_specs entry."""
+    d = domain(spec["n"], T0=spec["T0"], bubbles=[(0.0, 0.0, spec["radius"])],
+               mach=spec["mach"], bc=spec["bc"], li=ic.interface_length(spec["T0"], BATCH_WE),
+               we=BATCH_WE)
+    d["radius"] = spec["radius"]
+    return d
+
+
+def batched_domains(seed, count=64, sizes=tuple(range(128, 513, 64))):
+    """Batched FP64: `count` independent domains, n uniform in
+    {128, 192, ..., 512} (square), T0 in U[0.90, 0.99], bubble radius in
+    U[0.05, 0.2], boundary kind uniform over wall / periodic / open, flow
+    Mach in U[0, 0.1] for open domains (wall and periodic domains at rest).
+    The bubbles have the equilibrium interface width at T0 for We =
+    BATCH_WE (ic.interface_length); solve them with batch_params()."""
+    return [batched_domain(sp) for sp in batched_specs(seed, count, sizes)]
 
 
 SERVED_KINDS = ("wall_S_reflection", "hedstrom_xy")

@@ -222,20 +222,25 @@ DIM2D_API int dim2d_destroy(dim2d_handle *h);
 /* No counterpart in the reference.  The RK3 time step for callers that
  * cannot allocate device memory -- hosts whose HBM is handed out by their
  * own pool or arena, or time-stepping loops that must not call cudaMalloc
- * because it synchronises the device.  Same stages and boundary passes as
- * dim2d_step; the caller passes the field as a device pointer `nodes`
- * (Fortran layout nodes(nx,ny,4), ghosts included, updated in place) and
- * x_map/y_map as host arrays.  The two stage copies live in one
+ * because it synchronises the device.  The stages and boundary passes of
+ * dim2d_step for the two configurations without a node boundary pass:
+ * periodic_xy and hedstrom_xy (any other bc_choice / bc_type returns
+ * DIM2D_ERR_UNSUPPORTED).  The caller passes the field as a device pointer
+ * `nodes` (Fortran layout nodes(nx,ny,4), ghosts included, updated in
+ * place) and x_map/y_map as host arrays.  The two stage copies live in one
  * file-scope __device__ array of 2 x 4 x DIM2D_NOALLOC_MAX_CELLS doubles
  * (16 MiB), held on every GPU that loads the library until exit; larger
  * fields (nx*ny > DIM2D_NOALLOC_MAX_CELLS) are rejected with
  * DIM2D_ERR_ARG.  Nothing is allocated: no cudaMalloc / cudaFree.  All
  * calls on a device share that array and it keeps the last call's
  * contents (each call clears what it uses first); calls that overlap on
- * the GPU race on it, so order them on one stream.  The first call on a
- * device looks up the array's address with that device current: make it
- * before any stream capture.  `stream` is a cudaStream_t (NULL = legacy
- * default stream); the call returns without synchronising. */
+ * the GPU race on it, so order them on one stream.  The first call in a
+ * CUDA context looks up the array's address with that context current and
+ * keeps it for that context (a new context, e.g. after cudaDeviceReset,
+ * gets its own lookup): make that first call before any stream capture.
+ * `stream` is a cudaStream_t (NULL = legacy default stream); the call
+ * returns without synchronising.  After a non-zero return the contents of
+ * `nodes` are undefined. */
 #define DIM2D_NOALLOC_MAX_CELLS 262144
 DIM2D_API int dim2d_step_noalloc(const dim2d_params *p, int nx, int ny, const int bc_choice[8],
                                  const int bc_type[8], const int bc_order[8], double *nodes,

@@ -50,6 +50,39 @@ def build():
 
 
 _lib = None
+_fast = None
+
+
+def _cpu_key():
+    """Short key of this host's CPU model (a -march=native build is only
+    valid on the CPU it was built for)."""
+    import hashlib
+    import platform
+    model = platform.machine()
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith(("model name", "flags")):
+                    model += line
+    except OSError:
+        pass
+    return hashlib.sha1(model.encode()).hexdigest()[:12]
+
+
+def fast_lib():
+    """The timing build of the same sources (-O3 -march=native, same
+    rounding order), compiled on first use for this host's CPU.  Used only
+    to time the CPU baseline; the -O2 build (lib()) is the checker."""
+    global _fast
+    if _fast is None:
+        path = os.path.join(HERE, "_build", "fast_" + _cpu_key(), "liboracle_fast.so")
+        if not os.path.exists(path):
+            subprocess.check_call(["make", "-s", "-C", HERE, "fast",
+                                   "FAST_LIB=" + os.path.relpath(path, HERE)])
+        _fast = _declare(ctypes.CDLL(path))
+        p = get_params()  # the constants set on the checker build
+        _fast.orc_set_params(ctypes.byref(p))
+    return _fast
 
 
 def lib():
@@ -57,40 +90,44 @@ def lib():
     if _lib is None:
         if not os.path.exists(LIB_PATH):
             build()
-        L = ctypes.CDLL(LIB_PATH)
-        L.orc_sd_operator.restype = ctypes.c_double
-        L.orc_sd_operator.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
-                                      ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double]
-        L.orc_flux_function.restype = ctypes.c_double
-        L.orc_flux_function.argtypes = [ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
-                                        ctypes.c_int, ctypes.c_int, ctypes.c_double,
-                                        ctypes.c_double]
-        L.orc_classical_pressure_local.restype = ctypes.c_double
-        L.orc_classical_pressure_local.argtypes = [_dp]
-        L.orc_speed_of_sound.restype = ctypes.c_double
-        L.orc_speed_of_sound.argtypes = [_dp]
-        L.orc_compute_time_dev.restype = None
-        L.orc_compute_time_dev.argtypes = [ctypes.POINTER(Cfg), ctypes.c_double, _dp, _dp, _dp, _dp]
-        L.orc_apply_bc_on_nodes.restype = None
-        L.orc_apply_bc_on_nodes.argtypes = [ctypes.POINTER(Cfg), ctypes.c_double, _dp, _dp, _dp, _dp]
-        L.orc_integrate.restype = ctypes.c_int
-        L.orc_integrate.argtypes = [ctypes.POINTER(Cfg), _dp, _dp, _dp,
-                                    ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.c_int]
-        L.orc_ini_coordinates.restype = None
-        L.orc_ini_coordinates.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 4 + [_dp, _dp]
-        L.orc_set_params.argtypes = [ctypes.POINTER(Params)]
-        L.orc_get_params.argtypes = [ctypes.POINTER(Params)]
-        L.orc_set_threads.argtypes = [ctypes.c_int]
-        L.orc_debug_real.restype = ctypes.c_double
-        _ip = ctypes.POINTER(ctypes.c_int)
-        L.orc_compute_time_dev_masked.restype = None
-        L.orc_compute_time_dev_masked.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _ip,
-                                                  ctypes.c_double, ctypes.c_double, _ip, _ip, _dp]
-        L.orc_rk_stage_masked.restype = None
-        L.orc_rk_stage_masked.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp,
-                                          _ip, ctypes.c_double, _ip, _ip]
-        _lib = L
+        _lib = _declare(ctypes.CDLL(LIB_PATH))
     return _lib
+
+
+def _declare(L):
+    """Declare the C signatures on a loaded oracle library."""
+    L.orc_sd_operator.restype = ctypes.c_double
+    L.orc_sd_operator.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+    L.orc_flux_function.restype = ctypes.c_double
+    L.orc_flux_function.argtypes = [ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                    ctypes.c_double]
+    L.orc_classical_pressure_local.restype = ctypes.c_double
+    L.orc_classical_pressure_local.argtypes = [_dp]
+    L.orc_speed_of_sound.restype = ctypes.c_double
+    L.orc_speed_of_sound.argtypes = [_dp]
+    L.orc_compute_time_dev.restype = None
+    L.orc_compute_time_dev.argtypes = [ctypes.POINTER(Cfg), ctypes.c_double, _dp, _dp, _dp, _dp]
+    L.orc_apply_bc_on_nodes.restype = None
+    L.orc_apply_bc_on_nodes.argtypes = [ctypes.POINTER(Cfg), ctypes.c_double, _dp, _dp, _dp, _dp]
+    L.orc_integrate.restype = ctypes.c_int
+    L.orc_integrate.argtypes = [ctypes.POINTER(Cfg), _dp, _dp, _dp,
+                                ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.c_int]
+    L.orc_ini_coordinates.restype = None
+    L.orc_ini_coordinates.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 4 + [_dp, _dp]
+    L.orc_set_params.argtypes = [ctypes.POINTER(Params)]
+    L.orc_get_params.argtypes = [ctypes.POINTER(Params)]
+    L.orc_set_threads.argtypes = [ctypes.c_int]
+    L.orc_debug_real.restype = ctypes.c_double
+    _ip = ctypes.POINTER(ctypes.c_int)
+    L.orc_compute_time_dev_masked.restype = None
+    L.orc_compute_time_dev_masked.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _ip,
+                                              ctypes.c_double, ctypes.c_double, _ip, _ip, _dp]
+    L.orc_rk_stage_masked.restype = None
+    L.orc_rk_stage_masked.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp,
+                                      _ip, ctypes.c_double, _ip, _ip]
+    return L
 
 
 def ptr(a):
@@ -109,6 +146,8 @@ def set_params(**kw):
     for k, v in kw.items():
         setattr(p, k, v)
     lib().orc_set_params(ctypes.byref(p))
+    if _fast is not None:
+        _fast.orc_set_params(ctypes.byref(p))
     return p
 
 
@@ -146,11 +185,13 @@ def apply_bc_on_nodes(cfg, t, x_map, y_map, nodes_tmp, nodes):
                                 ptr(nodes))
 
 
-def integrate(cfg, nodes, x_map, y_map, t, dt, nsteps):
-    """Advance nodes in place by nsteps RK3 steps; returns the new time."""
+def integrate(cfg, nodes, x_map, y_map, t, dt, nsteps, fast=False):
+    """Advance nodes in place by nsteps RK3 steps; returns the new time.
+    fast: on the -O3 -march=native timing build (same results)."""
     tt = ctypes.c_double(t)
-    rc = lib().orc_integrate(ctypes.byref(cfg), ptr(nodes), ptr(x_map), ptr(y_map),
-                             ctypes.byref(tt), dt, nsteps)
+    L = fast_lib() if fast else lib()
+    rc = L.orc_integrate(ctypes.byref(cfg), ptr(nodes), ptr(x_map), ptr(y_map),
+                         ctypes.byref(tt), dt, nsteps)
     if rc != 0:
         raise RuntimeError("oracle integrate failed: %d" % rc)
     return tt.value

@@ -5,8 +5,8 @@ This script reads those programs AS TEXT (it compiles and runs nothing) and
 writes the inputs and expected values to small JSON files next to it, so the
 tests can pin the oracle without access to the reference tree.
 
-Usage:  python tests/golden/make_golden.py [reference_root]
-(default reference_root: /root/reference)
+Usage:  python tests/golden/make_golden.py <reference_root>
+(the root of a checkout of the reference project; required)
 
 Sources:
   src/test_files/test_augeanstables/test_mattsson_operators.f
@@ -264,7 +264,9 @@ def wall(ref):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2 or not os.path.isdir(os.path.join(sys.argv[1], "src")):
+        sys.exit("usage: python tests/golden/make_golden.py <reference_root>")
+    ref = sys.argv[1]
     out = {
         "mattsson_operators.json": mattsson(ref),
         "dim2d_fluxes.json": dim2d_fluxes(ref),

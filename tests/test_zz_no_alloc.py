@@ -6,8 +6,10 @@ dim2d_step_noalloc runs the same RK3 stages with its stage copies in a
 fixed file-scope device array.  This test checks, through the C ABI, that
 two calls in a row give the same state as the allocating entry point
 (dim2d_create / dim2d_upload / dim2d_step / dim2d_download), within the
-1e-12 normwise tolerance of the one-step parity tests, and that fields
-larger than the fixed limit are refused.
+1e-12 normwise tolerance of the one-step parity tests, for both accepted
+configurations (periodic_xy, hedstrom_xy) at an even and an odd width, and
+that fields larger than the fixed limit and configurations with a node
+boundary pass are refused.
 
 The file sorts last so a run that stops at the first failure has run every
 other test before this one.
@@ -17,7 +19,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from tests.helpers import periodic_case, stable_dt
+from tests.helpers import open_case, periodic_case, stable_dt
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
@@ -44,43 +46,71 @@ def _rel(a, b):
     return max(out)
 
 
-def test_noalloc_matches_allocating_path_two_calls():
+def _case(preset, n, ny):
+    if preset == "periodic_xy":
+        nx, nyy, x_map, y_map, q = periodic_case(n, ny, seed=11)
+        # periodic ghosts as field%ini leaves them
+        px, py = nx - 4, nyy - 4
+        q[:, :, 0:2] = q[:, :, px:px + 2]
+        q[:, :, nx - 2:] = q[:, :, 2:4]
+        q[:, 0:2, :] = q[:, py:py + 2, :]
+        q[:, nyy - 2:, :] = q[:, 2:4, :]
+    else:
+        nx, nyy, x_map, y_map, q = open_case(n, ny, seed=12, radius=0.15)
+    return nx, nyy, x_map, y_map, np.ascontiguousarray(q)
+
+
+# an even and an odd width: the caller's pitch is nx, so the odd one puts
+# every other row off a 16-byte boundary
+@pytest.mark.parametrize("preset", ["periodic_xy", "hedstrom_xy"])
+@pytest.mark.parametrize("n,ny", [(60, 44), (61, 44)])
+def test_noalloc_matches_allocating_path_two_calls(preset, n, ny):
     import torch
     F, L = _lib()
-    nx, ny, x_map, y_map, q = periodic_case(60, 44, seed=11)
-    # periodic ghosts as field%ini leaves them
-    px, py = nx - 4, ny - 4
-    q[:, :, 0:2] = q[:, :, px:px + 2]
-    q[:, :, nx - 2:] = q[:, :, 2:4]
-    q[:, 0:2, :] = q[:, py:py + 2, :]
-    q[:, ny - 2:, :] = q[:, 2:4, :]
+    nx, ny, x_map, y_map, q = _case(preset, n, ny)
     dt = stable_dt(q, x_map, y_map)
     steps = (5, 4)  # odd then even: the result leaves the scratch both ways
 
     # reference: the allocating entry points
     want = []
-    with F.Field(nx, ny, bc="periodic_xy") as fld:
+    with F.Field(nx, ny, bc=preset) as fld:
         fld.ini(q, x_map, y_map)
-        for n in steps:
-            fld.integrate(dt, n)
+        for n_ in steps:
+            fld.integrate(dt, n_)
             want.append(fld.download())
 
     # the no-allocation entry point, on a caller-owned device buffer
     p = F.default_params()
-    bc_choice, bc_type, bc_order = F._preset("periodic_xy")
+    bc_choice, bc_type, bc_order = F._preset(preset)
     arr = ctypes.c_int * 8
     dev = torch.from_numpy(q.copy()).cuda()
     stream = torch.cuda.current_stream()
-    for n, ref in zip(steps, want):
+    for n_, ref in zip(steps, want):
         rc = L.dim2d_step_noalloc(ctypes.byref(p), nx, ny, arr(*bc_choice), arr(*bc_type),
                                   arr(*bc_order), ctypes.c_void_p(dev.data_ptr()),
-                                  F._ptr(x_map), F._ptr(y_map), dt, n,
+                                  F._ptr(x_map), F._ptr(y_map), dt, n_,
                                   ctypes.c_void_p(stream.cuda_stream))
         assert rc == 0, L.dim2d_last_error().decode()
         torch.cuda.synchronize()
         got = dev.cpu().numpy()
         assert np.isfinite(got).all()
+        # open fields integrate their ghost cells too: compare every cell
         assert _rel(got, ref) <= TOL
+
+
+def test_noalloc_refuses_configurations_with_a_node_pass():
+    import torch
+    F, L = _lib()
+    nx, ny, x_map, y_map, q = periodic_case(40, 36)
+    p = F.default_params()
+    bc_choice, bc_type, bc_order = F._preset("wall_S_reflection")
+    arr = ctypes.c_int * 8
+    dev = torch.from_numpy(q.copy()).cuda()
+    rc = L.dim2d_step_noalloc(ctypes.byref(p), nx, ny, arr(*bc_choice), arr(*bc_type),
+                              arr(*bc_order), ctypes.c_void_p(dev.data_ptr()), F._ptr(x_map),
+                              F._ptr(y_map), 1e-6, 1, None)
+    assert rc == 3  # DIM2D_ERR_UNSUPPORTED
+    assert np.array_equal(dev.cpu().numpy(), q)
 
 
 def test_noalloc_rejects_fields_beyond_the_limit():
