@@ -33,6 +33,10 @@ def _lib():
             "dim2d_batch_sync": (ctypes.c_int, [H]),
             "dim2d_batch_set_shape": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int]),
             "dim2d_batch_set_graphs": (ctypes.c_int, [H, ctypes.c_int]),
+            "dim2d_batch_set_persistent": (ctypes.c_int, [H, ctypes.c_int]),
+            "dim2d_batch_set_rows": (ctypes.c_int, [H, ctypes.c_int]),
+            "dim2d_batch_set_wait_limit": (ctypes.c_int, [H, ctypes.c_double]),
+            "dim2d_batch_withhold_item": (ctypes.c_int, [H, ctypes.c_longlong]),
             "dim2d_batch_autotune": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_int), dp]),
             "dim2d_batch_size": (ctypes.c_int, [H]),
             "dim2d_batch_launch_count": (ctypes.c_longlong, [H]),
@@ -80,6 +84,21 @@ class Batch:
 
     def set_graphs(self, enable):
         _check(_lib().dim2d_batch_set_graphs(self._h, 1 if enable else 0))
+
+    def set_persistent(self, enable=True):
+        """Persistent mode: each step call is one persistent-kernel launch
+        per precision that advances every member (include/dim2d.h)."""
+        _check(_lib().dim2d_batch_set_persistent(self._h, int(bool(enable))))
+
+    def set_rows(self, rows):
+        _check(_lib().dim2d_batch_set_rows(self._h, int(rows)))
+
+    def set_wait_limit(self, seconds):
+        _check(_lib().dim2d_batch_set_wait_limit(self._h, float(seconds)))
+
+    def withhold_item(self, item):
+        """Tests of the bounded waits: never signal work item `item`."""
+        _check(_lib().dim2d_batch_withhold_item(self._h, int(item)))
 
     def set_stream(self, stream):
         _check(_lib().dim2d_batch_set_stream(self._h, ctypes.c_void_p(stream)))

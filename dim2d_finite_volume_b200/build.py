@@ -24,7 +24,8 @@ SOURCES = [
     "dim2d_strip.cu", "dim2d_batch.cu", "dim2d_server.cu",
     "dim2d_masked.cu",
 ]
-HEADERS = ["dim2d_physics.cuh", "dim2d_kernels.cuh", "dim2d_internal.h"]
+HEADERS = ["dim2d_physics.cuh", "dim2d_kernels.cuh", "dim2d_internal.h", "dim2d_open.cuh",
+           "dim2d_nodebc.cuh"]
 
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -196,4 +196,56 @@ struct NodeBcBatchArgs {
 // node boundary pass of every domain in P; fills P.d[].cta0
 cudaError_t launch_node_bc_batch(NodeBcBatchArgs& P, cudaStream_t s);
 
+// ---- persistent batched kernel (dim2d_strip.cu): one launch advances
+// every domain of a batch (any mix of boundary kinds, one precision) by
+// nsteps RK3 steps.  Its warps take work items in order from one counter:
+// per step and stage, the open ghost cells and the strips of every domain,
+// then the node boundary passes.  An item waits until every earlier item
+// of its own domain has completed (a completion counter per domain), so
+// domains advance independently and no grid-wide barrier is needed; items
+// are taken in dependency order, so the warps that wait always wait on
+// items that running warps hold.  Waits are bounded (wait_ns); one that
+// runs out sets `error` and stops the launch.
+enum PItemType : int { PI_GHOST = 0, PI_STRIP = 1, PI_NODE = 2 };
+
+struct PDomain {
+  Field f;
+  double* buf[3];  // at launch: [0] = u^n, [1] = the other buffer of the pair, [2] = C
+  double dx, dy, rdx, rdy, dt, xmap0, ymap0;
+  int periodic, wall_s, open;                        // as StageArgs
+  int south_wall, corners_y, open_w, open_e, open_n;  // as NodeBcArgs
+  int sx;                                            // strips per row band
+  int per_step;                                      // items of the domain per step
+  unsigned int* status;                              // wall root status word
+};
+
+struct PItem {
+  int dom;
+  int type;   // PItemType
+  int stage;  // 1, 2, 3
+  int index;  // ghost: 32-cell group; strip: row band * sx + column strip; node: 32-cell group
+  int need;   // items of the domain, within the step, that must complete first
+};
+
+struct PersistArgs {
+  DimConst k;
+  WallConst wall;
+  const PDomain* dom;
+  const PItem* items;
+  long long items_per_step;
+  int nsteps;
+  int step0;                      // buffer parity of the first step (0: u^n in buf[0])
+  double dt_scale;                // 1, or 0 for the autotuner's dry steps
+  int h_rows;                     // rows per strip item
+  unsigned long long* next;       // item counter (zero at launch)
+  unsigned long long* done;       // per-domain completion counters (zero at launch)
+  unsigned int* ctl;              // [0] abort flag, [1] error word (bit 0: a wait ran out)
+  unsigned long long wait_ns;     // limit of one dependency wait
+  long long withhold;             // item whose completion is never signalled (tests; -1: none)
+};
+
+// launch the persistent kernel with as many CTAs as fit on the device;
+// *ctas receives that number
+cudaError_t launch_batch_persistent(const PersistArgs& P, bool mixed, cudaStream_t s, int* ctas);
+
 }  // namespace dim2d

@@ -30,6 +30,7 @@
 // cells (open_ghost_cell, one thread each): they take the first CTAs of the
 // grid, so their long dependent chains start first and overlap the strips.
 // Ghost and interior cells read the same input and write disjoint cells.
+#include "dim2d_nodebc.cuh"
 #include "dim2d_open.cuh"
 
 namespace dim2d {
@@ -395,19 +396,12 @@ __device__ __forceinline__ void y_face_mix(const StageArgs& a, const FluxCoefF& 
 // half_wall_S_open): ghost CTAs of the open sections, wall faces in the strips
 enum StripKind : int { K_PLAIN = 0, K_WALL = 1, K_OPEN = 2, K_WALL_OPEN = 3 };
 
-// grid: [ghost CTAs (K_OPEN only)] + sx * sy strip CTAs, x fastest
-// The work of strip CTA number b of one field (sx strips per row band).
-template <int H, int WPC, int MODE, bool WALL, bool MIX>
-__device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// The strip of one warp: columns c0 .. c0+29 (interior ones), rows y0 ..
+// y1-1, with ring slot `warp` of the CTA's shared memory.
+template <int MODE, bool WALL, bool MIX>
+__device__ __forceinline__ void strip_warp(const StageArgs& a, int c0, int y0, int y1, int warp) {
+  const int lane = threadIdx.x & 31;
   const Field f = a.f;
-  // MODE 2 (buffer-layer grid): strips over the border box, the first one
-  // starting at an even column so that the rows' 16-byte pairs stay aligned
-  const int c0 = (MODE == 2 ? (a.box_x0 & ~1) : BC) + (b % sx) * SW;
-  const int y0 = (MODE == 2 ? a.box_y0 : BC) + ((b / sx) * WPC + warp) * H;
-  const int ylast = MODE == 2 ? a.box_y1 : f.ny - BC - 1;
-  if (y0 > ylast) return;  // the whole warp leaves; no CTA barrier is used
-  const int y1 = min(y0 + H, ylast + 1);
   const int x = c0 + lane;
   const DimConst& k = a.k;
   const double qrdx = 0.25 * a.rdx, qrdy = 0.25 * a.rdy;
@@ -561,6 +555,20 @@ __device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
   cp_async_wait<0>();  // the copies of rows past the strip land before the warp exits
 }
 
+// grid: [ghost CTAs (K_OPEN only)] + sx * sy strip CTAs, x fastest
+// The work of strip CTA number b of one field (sx strips per row band).
+template <int H, int WPC, int MODE, bool WALL, bool MIX>
+__device__ __forceinline__ void strip_cta(const StageArgs& a, int b, int sx) {
+  const int warp = threadIdx.x >> 5;
+  // MODE 2 (buffer-layer grid): strips over the border box, the first one
+  // starting at an even column so that the rows' 16-byte pairs stay aligned
+  const int c0 = (MODE == 2 ? (a.box_x0 & ~1) : BC) + (b % sx) * SW;
+  const int y0 = (MODE == 2 ? a.box_y0 : BC) + ((b / sx) * WPC + warp) * H;
+  const int ylast = MODE == 2 ? a.box_y1 : a.f.ny - BC - 1;
+  if (y0 > ylast) return;  // the whole warp leaves; no CTA barrier is used
+  strip_warp<MODE, WALL, MIX>(a, c0, y0, min(y0 + H, ylast + 1), warp);
+}
+
 template <int H, int WPC, int MINB, int MODE, int KIND, bool MIX>
 __global__ void __launch_bounds__(32 * WPC, MINB) k_strip(StageArgs a, int ghost_ctas, int sx) {
   int b = blockIdx.x;
@@ -639,6 +647,139 @@ __global__ void __launch_bounds__(32 * WPC, MINB)
   const StageArgs a = batch_stage_args(P, i);
   strip_cta<H, WPC, 1, KIND == K_WALL || KIND == K_WALL_OPEN, MIX>(a, b - P.d[i].strip0,
                                                                      P.d[i].sx);
+}
+
+// ---- persistent batched kernel -----------------------------------------
+// Item it of a launch is item it % items_per_step of the per-step table, in
+// step it / items_per_step.  Buffer roles of step k (A = buf[0] holds u^n at
+// launch, B = buf[1]): u^n = A on even steps and B on odd steps, the other
+// one of the pair takes stages 1 and 3, C takes stage 2 -- the A/B swap of
+// rk3_step, step after step.
+constexpr int PW = 2;  // warps per CTA of the persistent kernel
+
+__device__ __forceinline__ unsigned long long load_acquire(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// wait until done >= target (every lane loads with acquire semantics);
+// false if the launch was stopped or the wait ran out (which stops it)
+__device__ bool wait_done(const PersistArgs& P, const unsigned long long* done,
+                          unsigned long long target) {
+  if (load_acquire(done) >= target) return true;
+  const unsigned long long t0 = global_ns();
+  unsigned ns = 64;
+  // the iteration cap (a few seconds of 2 us sleeps) bounds the wait even
+  // if the timer stalled
+  for (int it = 0; it < (1 << 21); it++) {
+    __nanosleep(ns);
+    if (ns < 2048) ns *= 2;
+    if (load_acquire(done) >= target) return true;
+    if (*(volatile unsigned int*)&P.ctl[0]) return false;
+    if (global_ns() - t0 > P.wait_ns) break;
+  }
+  atomicOr(&P.ctl[1], 1u);
+  atomicExch(&P.ctl[0], 1u);
+  return false;
+}
+
+__device__ __forceinline__ StageArgs persist_stage_args(const PersistArgs& P, const PDomain& d,
+                                                        int step, int st) {
+  const int odd = (P.step0 + step) & 1;
+  double* X = odd ? d.buf[1] : d.buf[0];  // u^n
+  double* Y = odd ? d.buf[0] : d.buf[1];
+  StageArgs a;
+  a.uin = st == 1 ? X : (st == 2 ? Y : d.buf[2]);
+  a.u0 = X;
+  a.uout = st == 2 ? d.buf[2] : Y;
+  a.f = d.f;
+  a.dx = d.dx;
+  a.dy = d.dy;
+  a.rdx = d.rdx;
+  a.rdy = d.rdy;
+  a.dt = d.dt * P.dt_scale;
+  a.b = st == 2 ? 0.75 : (st == 3 ? 1.0 / 3.0 : 0.0);  // rk3tvd_steps_module.f:225,444
+  a.stage = st;
+  a.periodic = d.periodic;
+  a.wall_w = a.wall_e = a.wall_n = 0;
+  a.wall_s = d.wall_s;
+  a.variant = 0;
+  a.open = d.open;
+  a.mixed = 0;
+  a.t = 0.0;
+  a.xmap0 = d.xmap0;
+  a.ymap0 = d.ymap0;
+  a.node_sides = 0;  // the item order already waits for the node pass
+  a.mask = nullptr;
+  a.box_x0 = a.box_x1 = a.box_y0 = a.box_y1 = 0;
+  a.wall = P.wall;
+  a.k = P.k;
+  return a;
+}
+
+__device__ __forceinline__ NodeBcArgs persist_node_args(const PersistArgs& P, const PDomain& d,
+                                                        int step, int st) {
+  const int odd = (P.step0 + step) & 1;
+  double* X = odd ? d.buf[1] : d.buf[0];
+  double* Y = odd ? d.buf[0] : d.buf[1];
+  NodeBcArgs a;
+  a.utmp = X;
+  a.u = st == 2 ? d.buf[2] : Y;
+  a.f = d.f;
+  a.dx = d.dx;
+  a.dy = d.dy;
+  a.rdx = d.rdx;
+  a.rdy = d.rdy;
+  a.t = 0.0;
+  a.xmap0 = d.xmap0;
+  a.ymap0 = d.ymap0;
+  a.south_wall = d.south_wall;
+  a.corners_y = d.corners_y;
+  a.open_w = d.open_w;
+  a.open_e = d.open_e;
+  a.open_n = d.open_n;
+  a.status = d.status;
+  a.wall = P.wall;
+  a.k = P.k;
+  return a;
+}
+
+template <bool MIX>
+__global__ void __launch_bounds__(32 * PW, 8) k_batch_persistent(const __grid_constant__ PersistArgs P) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned long long total = (unsigned long long)P.items_per_step * P.nsteps;
+  for (;;) {
+    unsigned long long it = 0;
+    if (lane == 0) it = atomicAdd(P.next, 1ull);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it >= total || *(volatile unsigned int*)&P.ctl[0]) break;
+    const int step = (int)(it / (unsigned long long)P.items_per_step);
+    const PItem item = P.items[it % (unsigned long long)P.items_per_step];
+    const PDomain& d = P.dom[item.dom];
+    const unsigned long long target =
+        (unsigned long long)step * (unsigned long long)d.per_step + (unsigned long long)item.need;
+    if (!wait_done(P, P.done + item.dom, target)) break;
+    if (item.type == PI_STRIP) {
+      const StageArgs a = persist_stage_args(P, d, step, item.stage);
+      const int c0 = BC + (item.index % d.sx) * SW;
+      const int y0 = BC + (item.index / d.sx) * P.h_rows;
+      strip_warp<1, true, MIX>(a, c0, y0, min(y0 + P.h_rows, d.f.ny - BC), warp);
+    } else if (item.type == PI_GHOST) {
+      open_ghost_cell(persist_stage_args(P, d, step, item.stage), item.index * 32 + lane, 1);
+    } else {
+      node_bc_cell(persist_node_args(P, d, step, item.stage), item.index * 32 + lane);
+    }
+    // every lane's stores are visible device-wide before the item counts as done
+    __threadfence();
+    __syncwarp();
+    if (lane == 0 && (long long)it != P.withhold) atomicAdd(P.done + item.dom, 1ull);
+  }
 }
 
 #undef ST
@@ -728,6 +869,24 @@ cudaError_t launch_strip_batch_shape(BatchStageArgs& P, int kind, bool mixed, cu
 }
 
 }  // namespace
+
+cudaError_t launch_batch_persistent(const PersistArgs& P, bool mixed, cudaStream_t s, int* ctas) {
+  const size_t smem = (size_t)PW * (mixed ? WARP_DOUBLES_MIX : WARP_DOUBLES) * sizeof(double);
+  const void* fn = mixed ? (const void*)k_batch_persistent<true> : (const void*)k_batch_persistent<false>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0, per_sm = 0;
+  e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * PW, smem);
+  if (e != cudaSuccess) return e;
+  const int n = sms * (per_sm > 0 ? per_sm : 1);
+  if (ctas) *ctas = n;
+  PersistArgs pa = P;
+  void* args[] = {&pa};
+  return cudaLaunchKernel(fn, dim3((unsigned)n), dim3(32 * PW), args, smem, s);
+}
 
 cudaError_t launch_strip_batch(BatchStageArgs& P, int kind, int shape, bool mixed,
                                cudaStream_t s) {

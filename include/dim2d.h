@@ -307,9 +307,32 @@ DIM2D_API int dim2d_batch_sync(dim2d_batch *b);
 /* strip shape (0..4 = dim2d_set_variant 1..5) of one group */
 DIM2D_API int dim2d_batch_set_shape(dim2d_batch *b, int group, int shape);
 DIM2D_API int dim2d_batch_set_graphs(dim2d_batch *b, int enable);
+/* Persistent mode (enable != 0): dim2d_batch_step(b, n) is one launch of a
+ * persistent kernel per precision (FP64, DIM2D_MIXED) that advances every
+ * member by n steps.  Its warps take work items from one queue -- per step
+ * and stage, the ghost cells of open sections and the strips of every
+ * member, then the node boundary passes -- and an item starts once every
+ * earlier item of its own field has completed, so fields of every boundary
+ * kind and size advance together without grid-wide barriers.  Results are
+ * those of the graph mode bit for bit (the same per-cell code).  Each wait
+ * is bounded (dim2d_batch_set_wait_limit, default 2 s); one that runs out
+ * stops the launch and dim2d_batch_sync returns DIM2D_ERR_TIMEOUT. */
+DIM2D_API int dim2d_batch_set_persistent(dim2d_batch *b, int enable);
+/* rows of one strip work item of the persistent kernel: 8, 16 (default) or
+ * 32; dim2d_batch_autotune picks it in persistent mode */
+DIM2D_API int dim2d_batch_set_rows(dim2d_batch *b, int rows);
+DIM2D_API int dim2d_batch_set_wait_limit(dim2d_batch *b, double seconds);
+/* For tests of the bounded waits: in the next persistent launches, the
+ * completion of work item `item` (an index into the launch's item order)
+ * is not signalled, so the items of its field that follow wait until the
+ * limit runs out; -1 (default) turns this off. */
+DIM2D_API int dim2d_batch_withhold_item(dim2d_batch *b, long long item);
 /* Autotuner: times dry steps (dt = 0, stage buffers only) of each group
  * for the 5 strip shapes and keeps the fastest; chosen[8] receives the
- * shapes, times_ms (optional) 8 x 5 dry-step times (0 for empty groups). */
+ * shapes, times_ms (optional) 8 x 5 dry-step times (0 for empty groups).
+ * In persistent mode it times dry launches with 8, 16 and 32 rows per
+ * strip item instead: chosen[g] receives the rows kept and times_ms[g*5 +
+ * 0..2] the three times, for every g. */
 DIM2D_API int dim2d_batch_autotune(dim2d_batch *b, int chosen[8], double *times_ms);
 DIM2D_API int dim2d_batch_size(const dim2d_batch *b);
 DIM2D_API long long dim2d_batch_launch_count(const dim2d_batch *b);
