@@ -398,33 +398,66 @@ def run_batched(a, stream, barrier, F, torch, flush):
             e1.synchronize()
             plain_ms += e0.elapsed_time(e1)
     barrier()
-    bt = Bm.Batch()
-    bt.set_stream(stream.cuda_stream)
-    for fld, d in zip(fields, doms):
-        bt.add(fld, d["dt"])
-    shapes, _ = bt.autotune()
-    cells = bt.cells
-    bt.step(3)
-    barrier()
-    n0 = bt.launches
-    batch_ms, per_block, bclocks = timed_batch_steps(bt, a.batch_steps, stream, torch)
-    barrier()
-    bt.sync()
-    launches = bt.launches - n0
-    bt.close()
-    total_steps = 3 + steps + 3 + a.batch_steps  # every step the FP64 fields took
+    total_steps = 3 + steps + 3 + a.batch_steps  # every step the FP64 fields take
+    modes = {}
+    for mode in ("graph", "persistent"):
+        if mode == "persistent":
+            graph_state = [fld.download() for fld in fields]
+            reinit(fields, doms)  # the same steps again, from the initial state
+        modes[mode] = batch_mode_run(a, Bm, fields, doms, mode, stream, barrier, torch,
+                                     warm=total_steps - a.batch_steps)
+    # same per-cell code in both modes: the states after the same steps agree
+    diff = max(float(np.abs(fld.download() - g).max()) for fld, g in zip(fields, graph_state))
+    best = min(modes, key=lambda m: modes[m]["ms"])
+    cells = modes[best]["cells"]
+    batch_ms, per_block, bclocks = modes[best]["ms"], modes[best]["blocks"], modes[best]["clocks"]
     out = {"cells_per_step": int(cells), "steps": a.batch_steps, "batch_ms": batch_ms,
+           "mode": best, "mode_ms": {m: modes[m]["ms"] for m in modes},
+           "mode_launches": {m: modes[m]["launches"] for m in modes},
+           "persistent_rows": modes["persistent"]["shapes"][0],
+           "persistent_vs_graph_max_abs_diff": diff,
            "we": workloads.BATCH_WE, "clocks": bclocks,
            "block_ms_per_step": [round(min(per_block), 4), round(max(per_block), 4)],
-           "plain_ms": plain_ms, "plain_steps": steps, "launches": int(launches),
+           "plain_ms": plain_ms, "plain_steps": steps,
+           "launches": int(modes[best]["launches"]),
            "plain_variants": {str(v): plain_variants.count(v) for v in sorted(set(plain_variants))},
-           "domains": len(doms), "shapes": shapes,
+           "domains": len(doms), "shapes": modes["graph"]["shapes"],
            "kinds": {k: sum(1 for d in doms if d["bc"] == k) for k in workloads.BATCH_KINDS}}
     if a.batch_mixed:
         out["mixed"] = run_batched_mixed(a, stream, barrier, F, Bm, torch, flush, doms, fields,
                                          total_steps)
     for fld in fields:
         fld.close()
+    return out
+
+
+def reinit(fields, doms):
+    """Every field back to its initial state (field%ini)."""
+    for fld, d in zip(fields, doms):
+        fld.ini(d["nodes"], d["x_map"], d["y_map"])
+        if d["bc"] not in ("periodic_xy", "hedstrom_xy"):
+            fld.apply_bc_on_nodes()
+
+
+def batch_mode_run(a, Bm, fields, doms, mode, stream, barrier, torch, warm):
+    """One batch of `fields` in `mode` (graph: a captured graph of batched
+    launches per step; persistent: one persistent-kernel launch per step
+    call), autotuned, `warm` untimed steps, then the timed steps."""
+    bt = Bm.Batch()
+    bt.set_stream(stream.cuda_stream)
+    bt.set_persistent(mode == "persistent")
+    for fld, d in zip(fields, doms):
+        bt.add(fld, d["dt"])
+    shapes, _ = bt.autotune()
+    bt.step(warm)
+    barrier()
+    n0 = bt.launches
+    ms, per_block, clocks = timed_batch_steps(bt, a.batch_steps, stream, torch)
+    barrier()
+    bt.sync()
+    out = {"ms": ms, "blocks": per_block, "clocks": clocks, "shapes": shapes,
+           "launches": bt.launches - n0, "cells": bt.cells}
+    bt.close()
     return out
 
 
@@ -468,20 +501,15 @@ def run_batched_mixed(a, stream, barrier, F, Bm, torch, flush, doms, fields64, t
         if d["bc"] not in ("periodic_xy", "hedstrom_xy"):
             fld.apply_bc_on_nodes()  # field%ini
         fields.append(fld)
-    bt = Bm.Batch()
-    bt.set_stream(stream.cuda_stream)
-    for fld, d in zip(fields, doms):
-        bt.add(fld, d["dt"])
-    shapes, _ = bt.autotune()
-    warm = total_steps - a.batch_steps
-    bt.step(warm)
-    barrier()
-    n0 = bt.launches
-    ms, per_block, mclocks = timed_batch_steps(bt, a.batch_steps, stream, torch)
-    barrier()
-    bt.sync()
-    launches = bt.launches - n0
-    bt.close()
+    modes = {}
+    for mode in ("graph", "persistent"):
+        if mode == "persistent":
+            reinit(fields, doms)
+        modes[mode] = batch_mode_run(a, Bm, fields, doms, mode, stream, barrier, torch,
+                                     warm=total_steps - a.batch_steps)
+    best = min(modes, key=lambda m: modes[m]["ms"])
+    ms, per_block, mclocks = modes[best]["ms"], modes[best]["blocks"], modes[best]["clocks"]
+    shapes, launches = modes[best]["shapes"], modes[best]["launches"]
     err = np.zeros(4)
     abs_err = np.zeros(4)
     scale = np.zeros(4)
@@ -499,6 +527,7 @@ def run_batched_mixed(a, stream, barrier, F, Bm, torch, flush, doms, fields64, t
             scale[v] = max(scale[v], float(np.abs(b_).max()))
         fm.close()
     return {"batch_ms": ms, "steps": a.batch_steps, "launches": int(launches), "shapes": shapes,
+            "mode": best, "mode_ms": {m: modes[m]["ms"] for m in modes},
             "steps_compared": total_steps, "rel_err_vs_fp64": [float(e) for e in err],
             "abs_err_vs_fp64": [float(e) for e in abs_err],
             "max_abs_fp64": [float(e) for e in scale], "clocks": mclocks,
@@ -863,15 +892,26 @@ def main():
             "steps": bres["steps"], "cells_per_step": bres["cells_per_step"],
             "kinds": bres["kinds"], "shapes": bres["shapes"],
             "gpu_launches": bres["launches"],
+            "mode": bres["mode"],
+            "mode_values": {m: whole_job_rate(bres["cells_per_step"], world, bres["steps"],
+                                              reduce_max([v], dist, "cuda")[0])
+                            for m, v in bres["mode_ms"].items()},
+            "mode_launches": bres["mode_launches"],
+            "persistent_rows": bres["persistent_rows"],
+            "persistent_vs_graph_max_abs_diff": bres["persistent_vs_graph_max_abs_diff"],
             "plain_per_field_value": pv,
             "plain_variants": bres["plain_variants"],
             "vs_plain_per_field": bv / pv,
             "roofline": {"bound": "hbm", "achieved": bv * BYTES_PER_CELL_UPDATE / 1e9,
                          "peak": peak_b, "unit": "GB/s",
                          "frac": bv * BYTES_PER_CELL_UPDATE / 1e9 / peak_b},
-            "timing": "CUDA events around blocks of 100 batched steps (each step one replay "
-                      "of the batch's step graph), no L2 flush: the batch's state is several "
-                      "times larger than L2; plain: the same fields stepped one after another, "
+            "timing": "CUDA events around blocks of 100 batched steps, no L2 flush: the "
+                      "batch's state is several times larger than L2.  Two modes from the same "
+                      "initial state, the faster one in value: graph = one replay of the "
+                      "batch's step graph (batched launches per stage and boundary kind) per "
+                      "step; persistent = one persistent-kernel launch per block (a dependency-"
+                      "ordered work queue over all domains).  plain: the same fields stepped "
+                      "one after another, "
                       "each by its own step graph with the stage-kernel variant its own "
                       "autotuner picked (plain_variants: variant -> fields), L2 flushed "
                       "between steps (outside the events)",
@@ -886,6 +926,10 @@ def main():
                             "pass / capillary third derivative / RK accumulation), one batch",
                 "value": mv, "unit": "cell-updates/s", "ms_per_step": tm / bm["steps"],
                 "steps": bm["steps"], "gpu_launches": bm["launches"], "shapes": bm["shapes"],
+                "mode": bm["mode"],
+                "mode_values": {m: whole_job_rate(bres["cells_per_step"], world, bm["steps"],
+                                                  reduce_max([v], dist, "cuda")[0])
+                                for m, v in bm["mode_ms"].items()},
                 "vs_fp64_batched": mv / bv, "vs_plain_per_field": mv / pv,
                 "roofline": {"bound": "hbm", "achieved": mv * BYTES_PER_CELL_UPDATE / 1e9,
                              "peak": peak_b, "unit": "GB/s",
