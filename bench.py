@@ -36,7 +36,8 @@ BYTES_PER_CELL_UPDATE = 256  # 3 stage writes + 3 stage reads + 2 reads of u^n, 
 L2_BYTES = 126 * 1024 * 1024
 # stage-kernel variants of the library (dim2d_set_variant)
 STAGE_KERNELS = ["k_interior<1> 32x8 tiles", "k_strip<8,4,4>", "k_strip<16,4,4>",
-                 "k_strip<16,4,5>", "k_strip<16,2,8>", "k_strip<16,8,2>"]
+                 "k_strip<16,4,5>", "k_strip<16,2,8>", "k_strip<16,8,2>",
+                 "k_batch_persistent (a whole RK3 step per launch)"]
 
 
 # presets with a wall on S: their CPU samples are the bottom rows (the wall)
@@ -954,17 +955,22 @@ def main():
     if rank == 0:
         peak, peak_kind = measured_peaks()
         ev_launch_ms = prof_ms / max(1, prof_n)
-        if launches == 3 * a.steps:
-            # every launch of the timed steps is a stage launch: the average
-            # launch duration over the timed region is at most step time / 3
+        # stage launches per step: 3, or 1 for the persistent kernel (a
+        # whole RK3 step per launch)
+        per_step = 1 if variant == 6 else 3
+        if launches == per_step * a.steps:
+            # every launch of the timed steps is a stage-kernel launch: the
+            # average launch duration over the timed region is at most step
+            # time / launches per step
             per_launch_ms = step_ms / launches
-            launch_timing = ("timed steps / stage launches (each timed step replays a graph of "
-                             "exactly 3 stage launches; inter-launch gaps included)")
+            launch_timing = ("timed steps / kernel launches (each timed step is exactly %d "
+                             "launch%s of the kernel; inter-launch gaps included)"
+                             % (per_step, "es" if per_step > 1 else ""))
         else:
             per_launch_ms = ev_launch_ms
             launch_timing = ("CUDA events around each stage launch over %d further steps "
                              "(stream launches of the same kernels)" % a.steps)
-        bytes_per_launch = cells * BYTES_PER_CELL_UPDATE / 3.0
+        bytes_per_launch = cells * BYTES_PER_CELL_UPDATE / float(per_step)
         achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
         tr = profile_traffic()
         line = {
@@ -980,11 +986,12 @@ def main():
             "replicas_per_gpu": 1,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
-                         "kernel": STAGE_KERNELS[variant] + " (fused RK3 stage)",
+                         "kernel": STAGE_KERNELS[variant] + (" (fused RK3 stage)" if variant != 6
+                                                             else ""),
                          "algorithmic_bytes_per_launch": bytes_per_launch,
                          "launch_ms": per_launch_ms, "launch_timing": launch_timing,
                          "launch_ms_events": ev_launch_ms,
-                         "traffic": (tr * cells if tr is not None else None)},
+                         "traffic": (tr * cells * 3 / per_step if tr is not None else None)},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s",
                     "h2d_bytes_per_step": int(hin.nbytes + w["x_map"].nbytes + w["y_map"].nbytes),
                     "d2h_bytes_per_step": int(hout.nbytes),

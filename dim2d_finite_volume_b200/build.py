@@ -22,7 +22,7 @@ SOURCES = [
     "dim2d_open.cu",
     "dim2d_nodebc.cu",
     "dim2d_strip.cu", "dim2d_batch.cu", "dim2d_server.cu",
-    "dim2d_masked.cu",
+    "dim2d_masked.cu", "dim2d_persist.cu",
 ]
 HEADERS = ["dim2d_physics.cuh", "dim2d_kernels.cuh", "dim2d_internal.h", "dim2d_open.cuh",
            "dim2d_nodebc.cuh"]

@@ -47,22 +47,6 @@ bool has_node_pass(int g) { return g % NKINDS == G_WALL || g % NKINDS == G_MIRRO
 bool is_mixed(int g) { return g >= NKINDS; }
 }  // namespace
 
-// Work tables of the persistent kernel for the members of one precision
-// (FP64 or DIM2D_MIXED): per-domain descriptors and the per-step item list
-// in device memory, the launch counters, and the device buffers' roles at
-// the time the tables were built (steps since then set the parity).
-struct PersistPlan {
-  std::vector<int> members;
-  PDomain* dom = nullptr;
-  PItem* items = nullptr;
-  unsigned long long* ctr = nullptr;  // [0] next item, [1..n] per-domain done counts
-  unsigned int* ctl = nullptr;        // [0] abort flag, [1] error word
-  long long items_per_step = 0;
-  int rows = 0;                       // rows per strip item the tables were built for
-  int ctas = 0;                       // CTAs of the last launch
-  bool valid = false;
-};
-
 struct dim2d_batch {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -250,158 +234,38 @@ int publish(dim2d_batch* b) {
   return e == cudaSuccess ? DIM2D_OK : cuda_error(e, "batch");
 }
 
-void free_plan(PersistPlan& pl) {
-  if (pl.dom) cudaFree(pl.dom);
-  if (pl.items) cudaFree(pl.items);
-  if (pl.ctr) cudaFree(pl.ctr);
-  if (pl.ctl) cudaFree(pl.ctl);
-  pl = PersistPlan();
-}
-
 void drop_plans(dim2d_batch* b) {
-  for (PersistPlan& pl : b->plan) free_plan(pl);
+  for (PersistPlan& pl : b->plan) persist_free(pl);
   b->pparity = 0;
 }
 
-NodeBcArgs node_args_of(const dim2d_handle* h) {
-  NodeBcArgs a{};
-  a.f = h->f;
-  a.south_wall = h->south_wall;
-  a.corners_y = h->corners_y;
-  a.open_w = h->open_w;
-  a.open_e = h->open_e;
-  a.open_n = h->open_n;
-  return a;
-}
-
-// Tables of the members of precision `cls` for strip items of `rows` rows:
-// per stage, the ghost-cell items of every open section, then the strips
-// (largest domains first), then the node boundary passes (wall domains
-// first); every item needs all earlier items of its domain in the step.
+// tables of the members of precision cls (0 FP64, 1 DIM2D_MIXED)
 int build_plan(dim2d_batch* b, int cls, int rows) {
-  PersistPlan& pl = b->plan[cls];
-  free_plan(pl);
+  std::vector<dim2d_handle*> hs;
+  std::vector<double> dts;
   for (size_t i = 0; i < b->m.size(); i++)
-    if ((b->m[i]->precision == DIM2D_MIXED) == (cls == 1)) pl.members.push_back((int)i);
-  pl.rows = rows;
-  if (pl.members.empty()) {
-    pl.valid = true;
-    return DIM2D_OK;
-  }
-  const int n = (int)pl.members.size();
-  std::vector<PDomain> dom(n);
-  std::vector<int> ng(n), ns(n), nn(n);
-  for (int j = 0; j < n; j++) {
-    const dim2d_handle* h = b->m[pl.members[j]];
-    PDomain& d = dom[j];
-    d.f = h->f;
-    d.buf[0] = h->A;
-    d.buf[1] = h->B;
-    d.buf[2] = h->C;
-    d.dx = h->dx;
-    d.dy = h->dy;
-    d.rdx = h->rdx;
-    d.rdy = h->rdy;
-    d.dt = b->dt[pl.members[j]];
-    d.xmap0 = h->xmap0;
-    d.ymap0 = h->ymap0;
-    d.periodic = h->periodic;
-    d.wall_s = h->south_wall;
-    d.open = h->open_mask;
-    d.south_wall = h->south_wall;
-    d.corners_y = h->corners_y;
-    d.open_w = h->open_w;
-    d.open_e = h->open_e;
-    d.open_n = h->open_n;
-    d.status = h->status;
-    d.sx = (h->f.nx - 2 * BC + 29) / 30;  // 30 interior columns per strip
-    const int sy = (h->f.ny - 2 * BC + rows - 1) / rows;
-    ng[j] = h->open_mask ? (open_ghost_count(h->f, h->open_mask) + 31) / 32 : 0;
-    ns[j] = d.sx * sy;
-    nn[j] = (h->periodic || h->open_all) ? 0 : (node_bc_count(node_args_of(h)) + 31) / 32;
-    d.per_step = 3 * (ng[j] + ns[j] + nn[j]);
-  }
-  std::vector<int> by_size(n), by_wall(n);
-  for (int j = 0; j < n; j++) by_size[j] = by_wall[j] = j;
-  std::stable_sort(by_size.begin(), by_size.end(), [&](int x, int y) { return ns[x] > ns[y]; });
-  std::stable_sort(by_wall.begin(), by_wall.end(),
-                   [&](int x, int y) { return dom[x].south_wall > dom[y].south_wall; });
-  std::vector<PItem> items;
-  for (int st = 1; st <= 3; st++) {
-    for (int j = 0; j < n; j++)
-      for (int q = 0; q < ng[j]; q++)
-        items.push_back(PItem{j, PI_GHOST, st, q, (st - 1) * (ng[j] + ns[j] + nn[j])});
-    for (int j : by_size)
-      for (int q = 0; q < ns[j]; q++)
-        items.push_back(PItem{j, PI_STRIP, st, q, (st - 1) * (ng[j] + ns[j] + nn[j])});
-    for (int j : by_wall)
-      for (int q = 0; q < nn[j]; q++)
-        items.push_back(PItem{j, PI_NODE, st, q, (st - 1) * (ng[j] + ns[j] + nn[j]) + ng[j] + ns[j]});
-  }
-  pl.items_per_step = (long long)items.size();
-  cudaError_t e = cudaMalloc(&pl.dom, sizeof(PDomain) * n);
-  if (e == cudaSuccess) e = cudaMalloc(&pl.items, sizeof(PItem) * items.size());
-  if (e == cudaSuccess) e = cudaMalloc(&pl.ctr, sizeof(unsigned long long) * (n + 1));
-  if (e == cudaSuccess) e = cudaMalloc(&pl.ctl, sizeof(unsigned int) * 2);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(pl.dom, dom.data(), sizeof(PDomain) * n, cudaMemcpyHostToDevice,
-                        b->stream);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(pl.items, items.data(), sizeof(PItem) * items.size(),
-                        cudaMemcpyHostToDevice, b->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(pl.ctl, 0, sizeof(unsigned int) * 2, b->stream);
-  // the host tables go out of scope: the copies must land first
-  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
-  if (e != cudaSuccess) {
-    free_plan(pl);
-    return cuda_error(e, "batch persistent tables");
-  }
-  pl.valid = true;
-  return DIM2D_OK;
-}
-
-// nsteps steps of the members of precision cls on stream s (dt_scale 0: a
-// dry step for the autotuner, which writes only the stage buffers)
-cudaError_t launch_plan(dim2d_batch* b, int cls, int nsteps, double dt_scale, cudaStream_t s) {
-  PersistPlan& pl = b->plan[cls];
-  if (pl.members.empty() || nsteps <= 0) return cudaSuccess;
-  const int n = (int)pl.members.size();
-  cudaError_t e = cudaMemsetAsync(pl.ctr, 0, sizeof(unsigned long long) * (n + 1), s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(pl.ctl, 0, sizeof(unsigned int), s);  // abort flag
-  if (e != cudaSuccess) return e;
-  const dim2d_handle* h0 = b->m[pl.members[0]];
-  PersistArgs P{};
-  P.k = h0->k;
-  P.wall = h0->wall;
-  P.dom = pl.dom;
-  P.items = pl.items;
-  P.items_per_step = pl.items_per_step;
-  P.nsteps = nsteps;
-  P.step0 = (int)(b->pparity & 1);
-  P.dt_scale = dt_scale;
-  P.h_rows = pl.rows;
-  P.next = pl.ctr;
-  P.done = pl.ctr + 1;
-  P.ctl = pl.ctl;
-  P.wait_ns = b->wait_ns;
-  P.withhold = b->withhold;
-  e = launch_batch_persistent(P, cls == 1, s, &pl.ctas);
-  b->launches++;
-  return e;
-}
-
-int ensure_plans(dim2d_batch* b) {
-  for (int cls = 0; cls < 2; cls++)
-    if (!b->plan[cls].valid || b->plan[cls].rows != b->rows) {
-      if (b->plan[0].valid || b->plan[1].valid) {
-        // tables of both classes share the buffer parity: rebuild both
-        drop_plans(b);
-        cls = -1;
-        continue;
-      }
-      int rc = build_plan(b, cls, b->rows);
-      if (rc) return rc;
+    if ((b->m[i]->precision == DIM2D_MIXED) == (cls == 1)) {
+      hs.push_back(b->m[i]);
+      dts.push_back(b->dt[i]);
     }
+  return persist_build(b->plan[cls], hs, dts, rows, b->stream);
+}
+
+// tables of both precisions for the current members and rows: kept while
+// both are valid for b->rows, else both rebuilt (they share the buffer
+// parity counted by b->pparity)
+int ensure_plans(dim2d_batch* b) {
+  bool current = true;
+  for (const PersistPlan& pl : b->plan) current = current && pl.valid && pl.rows == b->rows;
+  if (current) return DIM2D_OK;
+  drop_plans(b);
+  for (int cls = 0; cls < 2; cls++) {
+    int rc = build_plan(b, cls, b->rows);
+    if (rc) {
+      drop_plans(b);
+      return rc;
+    }
+  }
   return DIM2D_OK;
 }
 
@@ -410,10 +274,13 @@ int ensure_plans(dim2d_batch* b) {
 cudaError_t persistent_steps(dim2d_batch* b, int nsteps, double dt_scale) {
   cudaError_t e = cudaEventRecord(b->fork, b->stream);
   for (int cls = 0; cls < 2 && e == cudaSuccess; cls++) {
-    if (b->plan[cls].members.empty()) continue;
+    if (b->plan[cls].nfields == 0) continue;
     cudaStream_t s = b->side[cls];
     e = cudaStreamWaitEvent(s, b->fork, 0);
-    if (e == cudaSuccess) e = launch_plan(b, cls, nsteps, dt_scale, s);
+    if (e == cudaSuccess)
+      e = persist_launch(b->plan[cls], nsteps, (int)(b->pparity & 1), dt_scale, b->wait_ns,
+                         b->withhold, s);
+    if (e == cudaSuccess) b->launches++;
     if (e == cudaSuccess) e = cudaEventRecord(b->join[cls], s);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join[cls], 0);
   }
@@ -422,20 +289,10 @@ cudaError_t persistent_steps(dim2d_batch* b, int nsteps, double dt_scale) {
 
 // error words of the persistent launches since the last check (synchronous)
 int persistent_errors(dim2d_batch* b) {
-  unsigned int err = 0;
   for (PersistPlan& pl : b->plan) {
-    if (!pl.ctl) continue;
-    unsigned int w = 0;
-    cudaError_t e = cudaMemcpy(&w, pl.ctl + 1, sizeof w, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && w) e = cudaMemset(pl.ctl + 1, 0, sizeof(unsigned int));
-    if (e != cudaSuccess) return cuda_error(e, "batch error word");
-    err |= w;
+    int rc = persist_error(pl);
+    if (rc) return rc;
   }
-  if (err)
-    return set_error(DIM2D_ERR_TIMEOUT,
-                     "batch: a work item of the persistent kernel waited longer than the "
-                     "limit for the items before it (error word 0x%x); the launch stopped and "
-                     "the members' state is undefined", err);
   return DIM2D_OK;
 }
 

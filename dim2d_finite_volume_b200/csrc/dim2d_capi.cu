@@ -321,6 +321,10 @@ int dim2d_destroy(dim2d_handle* h) {
     cudaEventDestroy(h->copy_done);
   }
   drop_graphs(h);
+  if (h->pplan) {
+    persist_free(*h->pplan);
+    delete h->pplan;
+  }
   for (cudaEvent_t ev : h->prof_ev) cudaEventDestroy(ev);
   // pooled buffers are released in stream order, after the queued work
   auto release = [&](void* b) {
@@ -375,8 +379,10 @@ int dim2d_upload(dim2d_handle* h, const double* nodes, const double* x_map, cons
   if (!(dx > 0) || !(dy > 0)) return set_error(DIM2D_ERR_ARG, "upload: x_map/y_map not increasing");
   // captured step graphs hold dx, dy and the map origins as kernel
   // parameters: keep them only while those are unchanged
-  if (!h->uploaded || dx != h->dx || dy != h->dy || x_map[0] != h->xmap0 || y_map[0] != h->ymap0)
+  if (!h->uploaded || dx != h->dx || dy != h->dy || x_map[0] != h->xmap0 || y_map[0] != h->ymap0) {
     h->graph_dt = -1.0;
+    h->pdt = -1.0;  // and the persistent kernel's tables
+  }
   h->dx = dx;
   h->dy = dy;
   h->rdx = 1.0 / h->dx;
@@ -514,6 +520,8 @@ int dim2d_autotune(dim2d_handle* h, int* chosen, double* times_ms) {
     // writing only the stage buffers B and C (A, the state, is read only
     // and the buffers are not swapped)
     auto dry_step = [&]() -> cudaError_t {
+      if (v == PERSIST_VARIANT)
+        return persist_steps(h, 0.0, 1, 0.0) == DIM2D_OK ? cudaSuccess : cudaErrorLaunchFailure;
       const double* in[3] = {h->A, h->B, h->C};
       double* out[3] = {h->B, h->C, h->B};
       for (int st = 1; st <= 3; st++) {

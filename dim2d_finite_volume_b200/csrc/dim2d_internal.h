@@ -8,6 +8,28 @@
 #include "../../include/dim2d.h"
 #include "dim2d_kernels.cuh"
 
+// Work tables of the persistent kernel for a set of fields of one precision
+// (dim2d_persist.cu): per-field descriptors, the per-step item list and the
+// per-band strip+ghost item counts in device memory, and the launch
+// counters.  The tables hold the fields' buffers as they were when built;
+// launches pass the step parity since then.
+struct PersistPlan {
+  dim2d::PDomain* dom = nullptr;
+  dim2d::PItem* items = nullptr;
+  int* sg = nullptr;
+  unsigned long long* ctr = nullptr;  // [0] next item, band counters, node counters
+  unsigned int* ctl = nullptr;        // [0] abort flag, [1] error word
+  long long items_per_step = 0;
+  int nfields = 0;
+  int nbands = 0;
+  int rows = 0;   // rows per band / strip item
+  int ctas = 0;   // CTAs of the last launch
+  bool mixed = false;
+  bool valid = false;
+  dim2d::DimConst k{};
+  dim2d::WallConst wall{};
+};
+
 struct dim2d_handle {
   int device = 0;
   dim2d_params p{};
@@ -62,6 +84,11 @@ struct dim2d_handle {
   double graph_dt = -1.0;
   const double* graph_A[2] = {nullptr, nullptr};
   long long graph_launches[2] = {0, 0};  // kernel launches in one replay
+  // stage-kernel variant 6: the persistent kernel, tables built on first
+  // use (pplan), steps since then (pparity)
+  PersistPlan* pplan = nullptr;
+  dim2d::PDomain pdom0{};  // buffers the tables were built with
+  double pdt = -1.0;       // dt the tables hold (-1: rebuild)
   // live timing of the interior stage kernel (dim2d_profile)
   bool prof = false;
   std::vector<cudaEvent_t> prof_ev;  // start/stop pairs
@@ -105,6 +132,10 @@ int rk3_step(dim2d_handle* h, double dt);
 // nsteps RK3 steps; each step replays a captured CUDA graph when graphs are
 // enabled and the handle is not profiling
 int rk3_steps(dim2d_handle* h, double dt, int nsteps);
+// variant 6 (the persistent kernel): nsteps steps as one launch;
+// dt_scale 0 = dry step of the autotuner
+constexpr int PERSIST_VARIANT = 6;
+int persist_steps(dim2d_handle* h, double dt, int nsteps, double dt_scale);
 // the complete work of one stage (mode 1) or time derivative (mode 0): the
 // stage kernel and, on open fields where the stage kernel does not cover
 // them, the ghost-cell kernel; counts launches, profiles the stage kernel
@@ -118,3 +149,15 @@ void drop_graphs(dim2d_handle* h);
 // before work on h->stream writes `target`: wait for a pending
 // dim2d_download_async copy whose source it is
 cudaError_t wait_copy_if(dim2d_handle* h, const double* target);
+
+// dim2d_persist.cu
+void persist_free(PersistPlan& pl);
+int persist_build(PersistPlan& pl, const std::vector<dim2d_handle*>& hs,
+                  const std::vector<double>& dts, int rows, cudaStream_t s);
+// nsteps steps of every field of the plan (dt_scale 0: dry steps that
+// write only the stage buffers); step0 = steps taken since the build
+cudaError_t persist_launch(PersistPlan& pl, int nsteps, int step0, double dt_scale,
+                           unsigned long long wait_ns, long long withhold, cudaStream_t s);
+// reads and clears the plan's error word (synchronous): DIM2D_ERR_TIMEOUT
+// if a launch stopped at a wait that ran out
+int persist_error(PersistPlan& pl);

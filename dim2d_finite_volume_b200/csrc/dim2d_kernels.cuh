@@ -119,10 +119,14 @@ inline bool stage_uses_strip(const StageArgs& a) {
 }
 // strip shape of a stage launch (variant 1..5; mixed fields on variant 0
 // use shape 1)
-inline int strip_shape_of(const StageArgs& a) { return a.variant > 0 ? a.variant - 1 : 1; }
+inline int strip_shape_of(const StageArgs& a) {
+  return a.variant >= 1 && a.variant <= 5 ? a.variant - 1 : (a.variant == 6 ? 3 : 1);
+}
 // 1 if the stage launch of `a` also covers the open-boundary ghost cells
 inline bool stage_fuses_open(const StageArgs& a) { return a.open && stage_uses_strip(a); }
-constexpr int NUM_VARIANTS = 6;
+// variants 0..5 as above; 6 = the persistent kernel (a whole step per
+// launch, dim2d_persist.cu); its time derivative alone uses strip shape 3
+constexpr int NUM_VARIANTS = 7;
 // L(a.uin) of the interior cells into a.uout (stage fields ignored)
 cudaError_t launch_time_dev(const StageArgs& a, cudaStream_t s);
 // L(u) of a buffer-layer grid at its interior_pt points (StageArgs::mask):
@@ -199,13 +203,17 @@ cudaError_t launch_node_bc_batch(NodeBcBatchArgs& P, cudaStream_t s);
 // ---- persistent batched kernel (dim2d_strip.cu): one launch advances
 // every domain of a batch (any mix of boundary kinds, one precision) by
 // nsteps RK3 steps.  Its warps take work items in order from one counter:
-// per step and stage, the open ghost cells and the strips of every domain,
-// then the node boundary passes.  An item waits until every earlier item
-// of its own domain has completed (a completion counter per domain), so
-// domains advance independently and no grid-wide barrier is needed; items
-// are taken in dependency order, so the warps that wait always wait on
-// items that running warps hold.  Waits are bounded (wait_ns); one that
-// runs out sets `error` and stops the launch.
+// per step and stage, band by band, the open ghost cells and strips of every
+// domain's row band, then the node boundary passes.  Dependencies are
+// tracked per row band: a strip or ghost item of a band waits until the
+// previous stage is complete on that band and its two neighbours (the
+// stencil's reach; periodic fields wrap around) and, where the field has a
+// node pass, until the previous stage's node pass is complete; a node item
+// waits until its stage is complete on every band.  So stage s+1 starts on
+// a band while stage s still runs elsewhere, fields advance independently,
+// and no grid-wide barrier is needed.  Items are taken in dependency order,
+// so warps that wait always wait on items that running warps hold.  Waits
+// are bounded (wait_ns); one that runs out sets `error` and stops the launch.
 enum PItemType : int { PI_GHOST = 0, PI_STRIP = 1, PI_NODE = 2 };
 
 struct PDomain {
@@ -215,7 +223,9 @@ struct PDomain {
   int periodic, wall_s, open;                        // as StageArgs
   int south_wall, corners_y, open_w, open_e, open_n;  // as NodeBcArgs
   int sx;                                            // strips per row band
-  int per_step;                                      // items of the domain per step
+  int nb;                                            // row bands
+  int band0;                                         // first of its band counters
+  int nn;                                            // node items per stage (0: no pass)
   unsigned int* status;                              // wall root status word
 };
 
@@ -223,8 +233,10 @@ struct PItem {
   int dom;
   int type;   // PItemType
   int stage;  // 1, 2, 3
-  int index;  // ghost: 32-cell group; strip: row band * sx + column strip; node: 32-cell group
-  int need;   // items of the domain, within the step, that must complete first
+  int index;  // strip: band * sx + column strip; ghost: first cell (open_ghost_cell
+              // numbering); node: 32-cell group of node_bc_cell
+  int count;  // ghost: cells of the item (<= 32)
+  int band;   // row band (strip, ghost)
 };
 
 struct PersistArgs {
@@ -232,13 +244,15 @@ struct PersistArgs {
   WallConst wall;
   const PDomain* dom;
   const PItem* items;
+  const int* sg;                  // strip + ghost items per stage of each band
   long long items_per_step;
   int nsteps;
   int step0;                      // buffer parity of the first step (0: u^n in buf[0])
   double dt_scale;                // 1, or 0 for the autotuner's dry steps
-  int h_rows;                     // rows per strip item
+  int h_rows;                     // rows per strip item (= per band)
   unsigned long long* next;       // item counter (zero at launch)
-  unsigned long long* done;       // per-domain completion counters (zero at launch)
+  unsigned long long* done;       // per-band completion counters (zero at launch)
+  unsigned long long* ndone;      // per-domain node-item completion counters (zero at launch)
   unsigned int* ctl;              // [0] abort flag, [1] error word (bit 0: a wait ran out)
   unsigned long long wait_ns;     // limit of one dependency wait
   long long withhold;             // item whose completion is never signalled (tests; -1: none)

@@ -29,7 +29,14 @@
 #pragma once
 #include "dim2d_kernels.cuh"
 
-#ifdef __CUDA_ARCH__
+// Device loads go through the read-only (non-coherent) path, except in a
+// translation unit that defines DIM2D_COHERENT_LOADS: the persistent kernel
+// reads fields that other SMs rewrite during the same launch, so its loads
+// must be coherent (ld.global.cg, ordered by the acquire of its waits).
+#if defined(__CUDA_ARCH__) && defined(DIM2D_COHERENT_LOADS)
+#define NBC_LDG(p) __ldcg(p)
+#define NBC_ST(p, v) (*(p) = (v))
+#elif defined(__CUDA_ARCH__)
 #define NBC_LDG(p) __ldg(p)
 #define NBC_ST(p, v) (*(p) = (v))
 #elif defined(DIM2D_LDG_HOST)

@@ -27,7 +27,13 @@
 #pragma once
 #include "dim2d_kernels.cuh"
 
-#ifdef __CUDA_ARCH__
+// Device loads go through the read-only (non-coherent) path, except in a
+// translation unit that defines DIM2D_COHERENT_LOADS: the persistent kernel
+// reads fields that other SMs rewrite during the same launch, so its loads
+// must be coherent (ld.global.cg, ordered by the acquire of its waits).
+#if defined(__CUDA_ARCH__) && defined(DIM2D_COHERENT_LOADS)
+#define DIM2D_LDG(p) __ldcg(p)
+#elif defined(__CUDA_ARCH__)
 #define DIM2D_LDG(p) __ldg(p)
 #elif defined(DIM2D_LDG_HOST)
 #define DIM2D_LDG(p) DIM2D_LDG_HOST(p)  // host emulation with checked reads

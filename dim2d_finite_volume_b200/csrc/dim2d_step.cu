@@ -106,6 +106,10 @@ void prof_end(dim2d_handle* h) {
 // Read the wall status word (synchronising).  Non-zero = a wall ghost cell
 // had no bracketed / converged root, where the reference stops.
 int check_status(dim2d_handle* h) {
+  if (h->pplan) {  // a persistent launch that stopped at a wait that ran out
+    int rc = persist_error(*h->pplan);
+    if (rc) return rc;
+  }
   if (!h->south_wall || !h->status) return DIM2D_OK;
   unsigned int st = 0;
   cudaError_t e = cudaMemcpyAsync(&st, h->status, sizeof st, cudaMemcpyDeviceToHost, h->stream);
@@ -204,7 +208,57 @@ static int capture_step(dim2d_handle* h, double dt, int slot) {
   return DIM2D_OK;
 }
 
+// Stage-kernel variant 6: nsteps steps as one launch of the persistent
+// kernel (dim2d_persist.cu) over this field alone -- stages pipelined band
+// by band, no stage boundary across the field.  The tables are built on
+// first use for this dt and the field's buffers, and rebuilt when either
+// changes; dt_scale 0 makes the autotuner's dry step (stage buffers only,
+// no swap, no time advance).
+int persist_steps(dim2d_handle* h, double dt, int nsteps, double dt_scale) {
+  if (nsteps <= 0) return DIM2D_OK;
+  // the launch writes both buffers of the pair: pending copies land first
+  if (h->copy_pending) {
+    cudaError_t ew = cudaStreamWaitEvent(h->stream, h->copy_done, 0);
+    if (ew != cudaSuccess) return cuda_error(ew, "step");
+    h->copy_pending = false;
+  }
+  // a dry step keeps whatever dt the tables hold (its stages use dt * 0)
+  const double pdt = dt_scale == 0.0 ? (h->pplan && h->pdt >= 0.0 ? h->pdt : 0.0) : dt;
+  bool rebuild = !h->pplan || !h->pplan->valid || h->pdt != pdt;
+  int step0 = 0;
+  if (!rebuild) {
+    // the tables hold the buffers as built; A/B swap with every step
+    const PDomain& d0 = h->pdom0;
+    if (h->A == d0.buf[0] && h->B == d0.buf[1] && h->C == d0.buf[2]) step0 = 0;
+    else if (h->A == d0.buf[1] && h->B == d0.buf[0] && h->C == d0.buf[2]) step0 = 1;
+    else rebuild = true;
+  }
+  if (rebuild) {
+    if (!h->pplan) h->pplan = new PersistPlan();
+    std::vector<dim2d_handle*> hs{h};
+    std::vector<double> dts{pdt};
+    int rc = persist_build(*h->pplan, hs, dts, 16, h->stream);
+    if (rc) return rc;
+    h->pdt = pdt;
+    h->pdom0.buf[0] = h->A;
+    h->pdom0.buf[1] = h->B;
+    h->pdom0.buf[2] = h->C;
+    step0 = 0;
+  }
+  prof_begin(h);
+  cudaError_t e = persist_launch(*h->pplan, nsteps, step0, dt_scale, 2000000000ull, -1, h->stream);
+  prof_end(h);
+  if (e != cudaSuccess) return cuda_error(e, "persistent step");
+  h->launches++;
+  if (dt_scale != 0.0) {
+    if (nsteps & 1) std::swap(h->A, h->B);
+    h->t += nsteps * dt;  // field_class.f:70
+  }
+  return DIM2D_OK;
+}
+
 int rk3_steps(dim2d_handle* h, double dt, int nsteps) {
+  if (h->variant == PERSIST_VARIANT) return persist_steps(h, dt, nsteps, 1.0);
   const bool graphs = h->use_graphs && !h->prof;
   if (graphs && h->graph_dt != dt) {
     drop_graphs(h);

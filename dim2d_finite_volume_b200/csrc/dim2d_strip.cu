@@ -30,6 +30,9 @@
 // cells (open_ghost_cell, one thread each): they take the first CTAs of the
 // grid, so their long dependent chains start first and overlap the strips.
 // Ghost and interior cells read the same input and write disjoint cells.
+// the ghost-cell and node-pass code of this file runs inside the persistent
+// kernel, whose inputs change during the launch: coherent loads
+#define DIM2D_COHERENT_LOADS
 #include "dim2d_nodebc.cuh"
 #include "dim2d_open.cuh"
 
@@ -750,6 +753,12 @@ __device__ __forceinline__ NodeBcArgs persist_node_args(const PersistArgs& P, co
   return a;
 }
 
+// wait until band b of domain d has completed `inst` stage-instances
+__device__ __forceinline__ bool wait_band(const PersistArgs& P, const PDomain& d, int b,
+                                          unsigned long long inst) {
+  return wait_done(P, P.done + d.band0 + b, inst * (unsigned long long)P.sg[d.band0 + b]);
+}
+
 template <bool MIX>
 __global__ void __launch_bounds__(32 * PW, 8) k_batch_persistent(const __grid_constant__ PersistArgs P) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -762,23 +771,45 @@ __global__ void __launch_bounds__(32 * PW, 8) k_batch_persistent(const __grid_co
     const int step = (int)(it / (unsigned long long)P.items_per_step);
     const PItem item = P.items[it % (unsigned long long)P.items_per_step];
     const PDomain& d = P.dom[item.dom];
-    const unsigned long long target =
-        (unsigned long long)step * (unsigned long long)d.per_step + (unsigned long long)item.need;
-    if (!wait_done(P, P.done + item.dom, target)) break;
+    // stage-instances (3 per step) that precede this item's stage
+    const unsigned long long inst = 3ull * (unsigned long long)step + (unsigned long long)(item.stage - 1);
+    // every lane waits on every counter the item depends on (acquire loads),
+    // so each lane's reads are ordered after the producers' writes
+    bool ok = true;
+    if (item.type == PI_NODE) {
+      // this stage complete on every band of the field
+      for (int b = 0; b < d.nb && ok; b++) ok = wait_band(P, d, b, inst + 1);
+    } else {
+      // the previous stage complete on this band and its neighbours
+      const int b = item.band;
+      for (int o = -1; o <= 1 && ok; o++) {
+        int bb = b + o;
+        if (bb < 0 || bb >= d.nb) {
+          if (!d.periodic) continue;
+          bb = (bb + d.nb) % d.nb;  // ghost images wrap around
+        }
+        ok = wait_band(P, d, bb, inst);
+      }
+      // and the previous stage's node pass (its ghost cells)
+      if (ok && d.nn) ok = wait_done(P, P.ndone + item.dom, inst * (unsigned long long)d.nn);
+    }
+    if (!ok) break;
     if (item.type == PI_STRIP) {
       const StageArgs a = persist_stage_args(P, d, step, item.stage);
       const int c0 = BC + (item.index % d.sx) * SW;
-      const int y0 = BC + (item.index / d.sx) * P.h_rows;
+      const int y0 = BC + item.band * P.h_rows;
       strip_warp<1, true, MIX>(a, c0, y0, min(y0 + P.h_rows, d.f.ny - BC), warp);
     } else if (item.type == PI_GHOST) {
-      open_ghost_cell(persist_stage_args(P, d, step, item.stage), item.index * 32 + lane, 1);
+      if (lane < item.count)
+        open_ghost_cell(persist_stage_args(P, d, step, item.stage), item.index + lane, 1);
     } else {
       node_bc_cell(persist_node_args(P, d, step, item.stage), item.index * 32 + lane);
     }
     // every lane's stores are visible device-wide before the item counts as done
     __threadfence();
     __syncwarp();
-    if (lane == 0 && (long long)it != P.withhold) atomicAdd(P.done + item.dom, 1ull);
+    if (lane == 0 && (long long)it != P.withhold)
+      atomicAdd(item.type == PI_NODE ? P.ndone + item.dom : P.done + d.band0 + item.band, 1ull);
   }
 }
 

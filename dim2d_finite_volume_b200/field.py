@@ -346,7 +346,7 @@ class Field:
     def launches(self):
         return library().dim2d_launch_count(self._h)
 
-    NUM_VARIANTS = 6
+    NUM_VARIANTS = 7
 
     @property
     def variant(self):

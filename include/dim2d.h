@@ -204,9 +204,15 @@ DIM2D_API int dim2d_profile_read(dim2d_handle *h, double *ms, long long *launche
 /* No counterpart in the reference (its stage loops have one fixed shape).
  * Stage-kernel variant: 0 = 32x8-cell CTA tiles; 1..5 = warp-streaming
  * strips 30 columns wide with (rows per warp, warps per CTA, resident CTAs
- * per SM) = (8,4,4), (16,4,4), (16,4,5), (16,2,8), (16,8,2).  Every variant
- * evaluates the same face fluxes; results agree to rounding. */
-#define DIM2D_NUM_VARIANTS 6
+ * per SM) = (8,4,4), (16,4,4), (16,4,5), (16,2,8), (16,8,2); 6 = the
+ * persistent kernel of batches (dim2d_batch_set_persistent) over this field
+ * alone: each dim2d_step call is one launch whose warps take 16-row strips
+ * stage by stage, a band starting its next stage as soon as it and its
+ * neighbours have finished the previous one (no field-wide stage
+ * boundary); its tables are built on the first step with a new dt and
+ * kept while dt and the grid are unchanged.  Every variant evaluates the
+ * same face fluxes; results agree to rounding. */
+#define DIM2D_NUM_VARIANTS 7
 DIM2D_API int dim2d_set_variant(dim2d_handle *h, int variant);
 DIM2D_API int dim2d_get_variant(const dim2d_handle *h);
 /* Autotuner: times every variant on the resident field (dry RK3 steps with

@@ -26,7 +26,7 @@ from tests.test_open_emulation import MIXED, open_cells
 
 pytestmark = pytest.mark.gpu
 PRESETS = ["wall_S_open", "half_wall_S_open"]
-VARIANTS = list(range(6))
+VARIANTS = list(range(7))
 DEBUG_REAL = 9.9692099683868690e+36  # td_operators_class.f:150-154
 
 

@@ -12,7 +12,7 @@ from tests.helpers import normwise_rel_err, normwise_rel_err_all, open_case, per
 from tests.test_nodebc_emulation import defined_ghost_mask
 
 pytestmark = pytest.mark.gpu
-VARIANTS = list(range(6))
+VARIANTS = list(range(7))
 PRESETS = ["periodic_xy", "hedstrom_xy", "reflection_xy", "wall_S_reflection"]
 
 
@@ -128,7 +128,7 @@ def test_set_variant_rejects_out_of_range(F):
     nx, ny, x_map, y_map, q = periodic_case(24, 20)
     with F.Field(nx, ny, bc="periodic_xy") as fld:
         with pytest.raises(F.Dim2dError):
-            fld.variant = 6
+            fld.variant = 7
         with pytest.raises(F.Dim2dError):
             fld.variant = -1
         assert fld.variant == 0
