@@ -10,6 +10,28 @@
 // with the step parity (the A/B swap of rk3_step), so a launch passes the
 // parity of its first step relative to the buffers the tables were built
 // with.
+//
+// Why the band dependencies order every access (X = u^n of step k, Y the
+// other buffer of the pair, C; "(k,s,b)" = stage s of step k on band b;
+// strips read rows y0-2 .. y1+2, so a band reads its neighbours' rows):
+//   (k,1,b) reads X on b-1..b+1, writes Y on b;  (k,2,b) reads Y on
+//   b-1..b+1 and X on b, writes C on b;  (k,3,b) reads C on b-1..b+1 and X
+//   on b, writes Y on b.  Step k+1 swaps X and Y.
+//   * read after write: every reader of stage s waits for stage s-1 on its
+//     band and both neighbours -- the rows it reads;
+//   * (k,3,b) writes Y rows of band b, read by (k,2,b-1..b+1): it waits
+//     for exactly those;
+//   * (k+1,1,b) writes X rows of band b (the old u^n), read by (k,1,b+-1)
+//     and by (k,2,b), (k,3,b) as u^n: it waits for (k,3,b-1..b+1), which
+//     waited for (k,2,b-2..b+2), which waited for (k,1,b-3..b+3);
+//   * (k+1,2,b) writes C rows of band b, read by (k,3,b-1..b+1): it waits
+//     for (k+1,1,b-1..b+1), which waited for (k,3,b-2..b+2);
+//   * ghost images of periodic fields land in the opposite band: the
+//     neighbour sets wrap around, so the same arguments hold;
+//   * node passes write ghost cells of the stage output after the stage is
+//     complete on every band, and every item of the next stage waits for
+//     the whole pass; the wall pass reads u^n (ghost row 1 included), whose
+//     next writer, stage 1 of the next step, waits for that pass too.
 #include <algorithm>
 #include <vector>
 
