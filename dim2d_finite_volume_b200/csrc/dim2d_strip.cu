@@ -665,6 +665,14 @@ __device__ __forceinline__ unsigned long long load_acquire(const unsigned long l
   asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ unsigned long long load_relaxed(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void fence_acquire() {
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
+}
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -780,18 +788,33 @@ __global__ void __launch_bounds__(32 * PW, 8) k_batch_persistent(const __grid_co
       // this stage complete on every band of the field
       for (int b = 0; b < d.nb && ok; b++) ok = wait_band(P, d, b, inst + 1);
     } else {
-      // the previous stage complete on this band and its neighbours
-      const int b = item.band;
-      for (int o = -1; o <= 1 && ok; o++) {
-        int bb = b + o;
-        if (bb < 0 || bb >= d.nb) {
-          if (!d.periodic) continue;
-          bb = (bb + d.nb) % d.nb;  // ghost images wrap around
-        }
-        ok = wait_band(P, d, bb, inst);
+      // the previous stage complete on this band and its neighbours (ghost
+      // images of periodic fields wrap around), and the previous stage's
+      // node pass (its ghost cells)
+      int bands[3];
+      for (int o = -1; o <= 1; o++) {
+        int bb = item.band + o;
+        if (bb < 0 || bb >= d.nb) bb = d.periodic ? (bb + d.nb) % d.nb : item.band;
+        bands[o + 1] = bb;
       }
-      // and the previous stage's node pass (its ghost cells)
-      if (ok && d.nn) ok = wait_done(P, P.ndone + item.dom, inst * (unsigned long long)d.nn);
+      // the four counters read together with relaxed loads and, if they are
+      // all ready (the usual case), one acquire fence (the acquire pattern:
+      // strong reads, then fence.acq_rel) -- one round trip instead of four;
+      // otherwise waits, one counter at a time
+      const unsigned long long c0 = load_relaxed(P.done + d.band0 + bands[0]);
+      const unsigned long long c1 = load_relaxed(P.done + d.band0 + bands[1]);
+      const unsigned long long c2 = load_relaxed(P.done + d.band0 + bands[2]);
+      const unsigned long long cn = d.nn ? load_relaxed(P.ndone + item.dom) : 0ull;
+      const bool ready = c0 >= inst * (unsigned long long)P.sg[d.band0 + bands[0]] &&
+                         c1 >= inst * (unsigned long long)P.sg[d.band0 + bands[1]] &&
+                         c2 >= inst * (unsigned long long)P.sg[d.band0 + bands[2]] &&
+                         cn >= inst * (unsigned long long)d.nn;
+      if (ready) {
+        fence_acquire();
+      } else {
+        for (int o = 0; o < 3 && ok; o++) ok = wait_band(P, d, bands[o], inst);
+        if (ok && d.nn) ok = wait_done(P, P.ndone + item.dom, inst * (unsigned long long)d.nn);
+      }
     }
     if (!ok) break;
     if (item.type == PI_STRIP) {
@@ -805,11 +828,18 @@ __global__ void __launch_bounds__(32 * PW, 8) k_batch_persistent(const __grid_co
     } else {
       node_bc_cell(persist_node_args(P, d, step, item.stage), item.index * 32 + lane);
     }
-    // every lane's stores are visible device-wide before the item counts as done
+    // every lane's stores are visible device-wide before the item counts as
+    // done; the counter's address is looked up again from the item table
+    // rather than kept live across the work
     __threadfence();
     __syncwarp();
-    if (lane == 0 && (long long)it != P.withhold)
-      atomicAdd(item.type == PI_NODE ? P.ndone + item.dom : P.done + d.band0 + item.band, 1ull);
+    if (lane == 0 && (long long)it != P.withhold) {
+      const PItem& done_item = P.items[it % (unsigned long long)P.items_per_step];
+      atomicAdd(done_item.type == PI_NODE
+                    ? P.ndone + done_item.dom
+                    : P.done + P.dom[done_item.dom].band0 + done_item.band,
+                1ull);
+    }
   }
 }
 
