@@ -435,7 +435,8 @@ int dim2d_batch_step(dim2d_batch* b, int nsteps) {
     if (e != cudaSuccess) return cuda_error(e, "batch persistent step");
     b->pparity += nsteps;
     if (nsteps & 1) swap_members(b);
-    for (size_t i = 0; i < b->m.size(); i++) b->m[i]->t += nsteps * b->dt[i];  // field_class.f:70
+    for (size_t i = 0; i < b->m.size(); i++)  // field_class.f:70, step by step
+      for (int k = 0; k < nsteps; k++) b->m[i]->t += b->dt[i];
     return publish(b);
   }
   if (b->use_graphs && !b->graphs_valid) {

@@ -80,7 +80,7 @@ std::vector<GhostRun> ghost_runs(const dim2d_handle* h, int rows, int nb) {
       add(off, cells, nb - 1);
     } else {  // W or E edge: BC columns of ey cells each
       for (int b = 0; b < nb; b++) {
-        const int r0 = b * rows, n = std::min(rows, ey - r0);
+        const int r0 = b * rows, n = b == nb - 1 ? ey - r0 : rows;
         for (int col = 0; col < BC; col++) add(off + col * ey + r0, n, b);
       }
     }
@@ -90,6 +90,17 @@ std::vector<GhostRun> ghost_runs(const dim2d_handle* h, int rows, int nb) {
 }
 
 }  // namespace
+
+// Row bands of ey interior rows: ey / rows rounded up, except that a last
+// band of fewer than 2 rows joins the one before it (the last band then
+// has up to rows + 1 rows).  The two last interior rows are the sources of
+// a periodic field's ghost images across the domain; in one band, the
+// neighbour dependencies (with wrap-around) cover them.
+static int band_count(int ey, int rows) {
+  int nb = (ey + rows - 1) / rows;
+  if (nb > 1 && ey - (nb - 1) * rows < 2) nb--;
+  return nb;
+}
 
 void persist_free(PersistPlan& pl) {
   if (pl.dom) cudaFree(pl.dom);
@@ -143,7 +154,7 @@ int persist_build(PersistPlan& pl, const std::vector<dim2d_handle*>& hs,
     d.open_n = h->open_n;
     d.status = h->status;
     d.sx = (h->f.nx - 2 * BC + 29) / 30;  // 30 interior columns per strip
-    d.nb = (h->f.ny - 2 * BC + rows - 1) / rows;
+    d.nb = band_count(h->f.ny - 2 * BC, rows);
     d.band0 = (int)sg.size();
     d.nn = (h->periodic || h->open_all) ? 0 : (node_bc_count(node_args_of(h)) + 31) / 32;
     ghosts[j] = ghost_runs(h, rows, d.nb);

@@ -252,7 +252,7 @@ int persist_steps(dim2d_handle* h, double dt, int nsteps, double dt_scale) {
   h->launches++;
   if (dt_scale != 0.0) {
     if (nsteps & 1) std::swap(h->A, h->B);
-    h->t += nsteps * dt;  // field_class.f:70
+    for (int s = 0; s < nsteps; s++) h->t += dt;  // field_class.f:70, step by step
   }
   return DIM2D_OK;
 }

@@ -73,10 +73,6 @@ __device__ __forceinline__ void cp_async16(double* smem, const double* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
-__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
@@ -120,11 +116,19 @@ __device__ __forceinline__ void async_row(const StageArgs& a, int c0, int row, i
   }
 }
 
-// u^n of row y at the lane's cell (clamped column) into the u^n ring row un
-__device__ __forceinline__ void async_un(const StageArgs& a, int x, int y, int un) {
-  const size_t go = (size_t)y * a.f.pitch + min(x, a.f.nx - 1 - BC);
+// u^n of row y, columns c0 .. c0+31, into the u^n ring row at offset un
+// (which includes the lane): lane p < 16 copies the 16-byte pair of columns
+// c0+2p, c0+2p+1 of the 4 planes through L2 (cp.async.cg; the persistent
+// kernel rereads u^n buffers that other SMs rewrite within its launch, and
+// the L2 path is coherent).  Addresses clamped to the pitch like async_row.
+__device__ __forceinline__ void async_un(const StageArgs& a, int c0, int y, int un, int lane) {
+  if (lane < 16) {
+    const int xp = min(c0 + 2 * lane, a.f.pitch - 2);
+    const double* src = a.u0 + (size_t)y * a.f.pitch + xp;
+    double* dst = g_ring + (un - lane) + 2 * lane;
 #pragma unroll
-  for (int v = 0; v < 4; v++) cp_async8(g_ring + un + v * 32, a.u0 + go + v * a.f.plane);
+    for (int v = 0; v < 4; v++) cp_async16(dst + v * 32, src + v * a.f.plane);
+  }
 }
 
 // node quantities of column c0-1+lane of one row: sm/s0/sp = state rows
@@ -455,7 +459,7 @@ __device__ __forceinline__ void strip_warp(const StageArgs& a, int c0, int y0, i
   else y_face<WALL>(a, s2, s0, um, u0, q1, q0, x, y0 - 1, Gb);
   __syncwarp();  // rows y0-2 and y0-1 are no longer read
   async_row(a, c0, y0 + 2, lane, s2);
-  if (need_un) async_un(a, x, y0, un0);
+  if (need_un) async_un(a, c0, y0, un0, lane);
   cp_async_commit();
 
   const bool active = lane < SW && x <= f.nx - 1 - BC &&
@@ -473,7 +477,7 @@ __device__ __forceinline__ void strip_warp(const StageArgs& a, int c0, int y0, i
 #pragma unroll 1
   for (int y = y0; y < y1; y++) {
     async_row(a, c0, y + 3, lane, s3);  // next row: lands during this one
-    if (need_un) async_un(a, x, y + 1, un1);
+    if (need_un) async_un(a, c0, y + 1, un1, lane);
     cp_async_commit();
     cp_async_wait<1>();  // all but the group just issued: rows y+2, u^n(y)
     __syncwarp();
@@ -816,24 +820,31 @@ __global__ void __launch_bounds__(32 * PW, 8) k_batch_persistent(const __grid_co
         if (ok && d.nn) ok = wait_done(P, P.ndone + item.dom, inst * (unsigned long long)d.nn);
       }
     }
-    if (!ok) break;
+    // a wait that ran out stops every lane (the launch is aborted)
+    if (!__all_sync(0xffffffffu, ok)) break;
     if (item.type == PI_STRIP) {
       const StageArgs a = persist_stage_args(P, d, step, item.stage);
       const int c0 = BC + (item.index % d.sx) * SW;
       const int y0 = BC + item.band * P.h_rows;
-      strip_warp<1, true, MIX>(a, c0, y0, min(y0 + P.h_rows, d.f.ny - BC), warp);
+      // the last band runs to the last interior row (it absorbs a remainder
+      // of fewer than 2 rows, so that the rows a periodic field images into
+      // the opposite ghost rows never span two bands)
+      const int y1 = item.band == d.nb - 1 ? d.f.ny - BC : y0 + P.h_rows;
+      strip_warp<1, true, MIX>(a, c0, y0, y1, warp);
     } else if (item.type == PI_GHOST) {
       if (lane < item.count)
         open_ghost_cell(persist_stage_args(P, d, step, item.stage), item.index + lane, 1);
     } else {
       node_bc_cell(persist_node_args(P, d, step, item.stage), item.index * 32 + lane);
     }
-    // every lane's stores are visible device-wide before the item counts as
-    // done; the counter's address is looked up again from the item table
-    // rather than kept live across the work
+    // release: every lane's stores are performed device-wide (its fence),
+    // the warp barrier orders them before lane 0, whose fence (cumulative)
+    // precedes the counter increment.  The counter's address is looked up
+    // again from the item table rather than kept live across the work.
     __threadfence();
     __syncwarp();
     if (lane == 0 && (long long)it != P.withhold) {
+      __threadfence();
       const PItem& done_item = P.items[it % (unsigned long long)P.items_per_step];
       atomicAdd(done_item.type == PI_NODE
                     ? P.ndone + done_item.dom

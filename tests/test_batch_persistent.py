@@ -3,9 +3,11 @@ per precision advances every member by n steps, work items taken in
 dependency order, per-field completion counters instead of grid barriers.
 
 Checked against the graph mode of the same batch (same per-cell code:
-normwise <= 1e-13, and equal bit for bit is reported), against the oracle
-(<= 1e-10 after 30 steps), in mixed precision, across odd and even step
-counts (the A/B buffer parity), with the autotuner, and the bounded waits:
+FP64 normwise <= 1e-13, and equal bit for bit is reported; mixed precision
+<= 1e-6, as FP32 face arithmetic compiled into another kernel may round
+differently), against the oracle (<= 1e-10 after 30 steps), across odd and
+even step counts (the A/B buffer parity), ragged sizes whose last row band
+would hold a single row, with the autotuner, and the bounded waits:
 a work item whose completion is withheld makes the waits of the items
 after it run out, the launch stops, dim2d_batch_sync returns
 DIM2D_ERR_TIMEOUT, and the device stays usable."""
@@ -86,11 +88,14 @@ def test_persistent_matches_oracle(oracle, F, B, cases):
         assert np.all(_err(g, ref, p) <= 1e-10), (p, _err(g, ref, p))
 
 
+MIXED_TOL = 1e-6
+
+
 def test_persistent_mixed_precision_matches_graph_mode(F, B, cases):
     ref = _run(F, B, cases, (6,), persistent=False, precision=F.MIXED)
     got = _run(F, B, cases, (6,), persistent=True, precision=F.MIXED)
     for (p, *_), (g, _), (r, _) in zip(cases, got, ref):
-        assert np.all(_err(g, r, p) <= 1e-13), (p, _err(g, r, p))
+        assert np.all(_err(g, r, p) <= MIXED_TOL), (p, _err(g, r, p))
 
 
 def test_persistent_both_precisions_in_one_batch(F, B, cases):
@@ -113,7 +118,18 @@ def test_persistent_both_precisions_in_one_batch(F, B, cases):
     refmx = _run(F, B, cases, (5,), persistent=False, precision=F.MIXED)
     for i, (p, *_) in enumerate(cases):
         r = (refmx if i % 2 else ref64)[i][0]
-        assert np.all(_err(got[i], r, p) <= 1e-13), (i, p)
+        assert np.all(_err(got[i], r, p) <= (MIXED_TOL if i % 2 else 1e-13)), (i, p)
+
+
+@pytest.mark.parametrize("rows", [8, 16, 32])
+def test_persistent_long_run_matches_graph_mode(F, B, cases, rows):
+    """200 steps in one launch: races between bands or stages would show up
+    as differences growing with the run; FP64 must stay at rounding level."""
+    ref = _run(F, B, cases, (200,), persistent=False)
+    got = _run(F, B, cases, (200,), persistent=True, rows=rows)
+    for (p, *_), (g, _), (r, _) in zip(cases, got, ref):
+        assert np.isfinite(g).all(), p
+        assert np.all(_err(g, r, p) <= 1e-11), (p, _err(g, r, p))
 
 
 def test_persistent_autotune_keeps_state(F, B, cases):
