@@ -404,11 +404,16 @@ def run_batched(a, stream, barrier, F, torch, flush):
     for mode in ("graph", "persistent"):
         if mode == "persistent":
             graph_state = [fld.download() for fld in fields]
-            reinit(fields, doms)  # the same steps again, from the initial state
+        reinit(fields, doms)  # both modes take the same steps from the initial state
         modes[mode] = batch_mode_run(a, Bm, fields, doms, mode, stream, barrier, torch,
                                      warm=total_steps - a.batch_steps)
     # same per-cell code in both modes: the states after the same steps agree
-    diff = max(float(np.abs(fld.download() - g).max()) for fld, g in zip(fields, graph_state))
+    # (normwise per field and variable; the open boundary amplifies rounding)
+    diff = 0.0
+    for fld, g in zip(fields, graph_state):
+        q = fld.download()
+        for v in range(4):
+            diff = max(diff, float(np.abs(q[v] - g[v]).max() / np.abs(g[v]).max()))
     best = min(modes, key=lambda m: modes[m]["ms"])
     cells = modes[best]["cells"]
     batch_ms, per_block, bclocks = modes[best]["ms"], modes[best]["blocks"], modes[best]["clocks"]
@@ -504,8 +509,7 @@ def run_batched_mixed(a, stream, barrier, F, Bm, torch, flush, doms, fields64, t
         fields.append(fld)
     modes = {}
     for mode in ("graph", "persistent"):
-        if mode == "persistent":
-            reinit(fields, doms)
+        reinit(fields, doms)
         modes[mode] = batch_mode_run(a, Bm, fields, doms, mode, stream, barrier, torch,
                                      warm=total_steps - a.batch_steps)
     best = min(modes, key=lambda m: modes[m]["ms"])

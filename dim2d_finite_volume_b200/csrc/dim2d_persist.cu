@@ -89,6 +89,22 @@ std::vector<GhostRun> ghost_runs(const dim2d_handle* h, int rows, int nb) {
   return out;
 }
 
+// 1 if strip q of band `band` reads a ghost cell that the field's node
+// pass writes (the strip reads columns c0-2 .. c0+31 and rows y0-2 ..
+// y1+2).  Only those strips wait for the node pass of the previous stage;
+// the cells the node pass reads (within two cells of its sides, and the
+// u^n rows next to a wall) are written only by such strips, so the others
+// need not wait for it either way.
+int strip_reads_node_ghosts(const dim2d_handle* h, const PDomain& d, int band, int q, int rows) {
+  const int sides = h->node_sides;
+  if (!sides) return 0;
+  const int c0 = BC + q * 30;
+  const int y0 = BC + band * rows;
+  const int y1 = band == d.nb - 1 ? h->f.ny - BC : y0 + rows;
+  return ((sides & NODE_W) && c0 - 2 < BC) || ((sides & NODE_E) && c0 + 31 >= h->f.nx - BC) ||
+         ((sides & NODE_S) && y0 - 2 < BC) || ((sides & NODE_N) && y1 + 2 >= h->f.ny - BC);
+}
+
 }  // namespace
 
 // Row bands of ey interior rows: ey / rows rounded up, except that a last
@@ -177,7 +193,8 @@ int persist_build(PersistPlan& pl, const std::vector<dim2d_handle*>& hs,
         for (const GhostRun& g : ghosts[j])
           if (g.band == band) items.push_back(PItem{j, PI_GHOST, st, g.first, g.count, band});
         for (int q = 0; q < dom[j].sx; q++)
-          items.push_back(PItem{j, PI_STRIP, st, band * dom[j].sx + q, 0, band});
+          items.push_back(PItem{j, PI_STRIP, st, band * dom[j].sx + q,
+                                strip_reads_node_ghosts(hs[j], dom[j], band, q, rows), band});
       }
     for (int j : by_wall)
       for (int q = 0; q < dom[j].nn; q++) items.push_back(PItem{j, PI_NODE, st, q, 0, 0});

@@ -785,43 +785,48 @@ __global__ void __launch_bounds__(32 * PW, 8) k_batch_persistent(const __grid_co
     const PDomain& d = P.dom[item.dom];
     // stage-instances (3 per step) that precede this item's stage
     const unsigned long long inst = 3ull * (unsigned long long)step + (unsigned long long)(item.stage - 1);
-    // every lane waits on every counter the item depends on (acquire loads),
-    // so each lane's reads are ordered after the producers' writes
+    // Lane 0 checks the counters the item depends on and fences (the
+    // acquire pattern); the warp barrier then orders that acquire before
+    // every lane's reads (the pattern of a cooperative grid barrier).
     bool ok = true;
-    if (item.type == PI_NODE) {
-      // this stage complete on every band of the field
-      for (int b = 0; b < d.nb && ok; b++) ok = wait_band(P, d, b, inst + 1);
-    } else {
-      // the previous stage complete on this band and its neighbours (ghost
-      // images of periodic fields wrap around), and the previous stage's
-      // node pass (its ghost cells)
-      int bands[3];
-      for (int o = -1; o <= 1; o++) {
-        int bb = item.band + o;
-        if (bb < 0 || bb >= d.nb) bb = d.periodic ? (bb + d.nb) % d.nb : item.band;
-        bands[o + 1] = bb;
-      }
-      // the four counters read together with relaxed loads and, if they are
-      // all ready (the usual case), one acquire fence (the acquire pattern:
-      // strong reads, then fence.acq_rel) -- one round trip instead of four;
-      // otherwise waits, one counter at a time
-      const unsigned long long c0 = load_relaxed(P.done + d.band0 + bands[0]);
-      const unsigned long long c1 = load_relaxed(P.done + d.band0 + bands[1]);
-      const unsigned long long c2 = load_relaxed(P.done + d.band0 + bands[2]);
-      const unsigned long long cn = d.nn ? load_relaxed(P.ndone + item.dom) : 0ull;
-      const bool ready = c0 >= inst * (unsigned long long)P.sg[d.band0 + bands[0]] &&
-                         c1 >= inst * (unsigned long long)P.sg[d.band0 + bands[1]] &&
-                         c2 >= inst * (unsigned long long)P.sg[d.band0 + bands[2]] &&
-                         cn >= inst * (unsigned long long)d.nn;
-      if (ready) {
-        fence_acquire();
+    if (lane == 0) {
+      if (item.type == PI_NODE) {
+        // this stage complete on every band of the field
+        for (int b = 0; b < d.nb && ok; b++) ok = wait_band(P, d, b, inst + 1);
       } else {
-        for (int o = 0; o < 3 && ok; o++) ok = wait_band(P, d, bands[o], inst);
-        if (ok && d.nn) ok = wait_done(P, P.ndone + item.dom, inst * (unsigned long long)d.nn);
+        // the previous stage complete on this band and its neighbours
+        // (ghost images of periodic fields wrap around), and, for items
+        // that read ghost cells the node pass writes (strips flag it in
+        // `count`), the previous stage's node pass
+        const bool need_node = d.nn && (item.type != PI_STRIP || item.count);
+        int bands[3];
+        for (int o = -1; o <= 1; o++) {
+          int bb = item.band + o;
+          if (bb < 0 || bb >= d.nb) bb = d.periodic ? (bb + d.nb) % d.nb : item.band;
+          bands[o + 1] = bb;
+        }
+        // the counters read together first (one round trip when they are
+        // ready, the usual case), then waited on one at a time
+        const unsigned long long c0 = load_relaxed(P.done + d.band0 + bands[0]);
+        const unsigned long long c1 = load_relaxed(P.done + d.band0 + bands[1]);
+        const unsigned long long c2 = load_relaxed(P.done + d.band0 + bands[2]);
+        const unsigned long long cn = need_node ? load_relaxed(P.ndone + item.dom) : 0ull;
+        const bool ready = c0 >= inst * (unsigned long long)P.sg[d.band0 + bands[0]] &&
+                           c1 >= inst * (unsigned long long)P.sg[d.band0 + bands[1]] &&
+                           c2 >= inst * (unsigned long long)P.sg[d.band0 + bands[2]] &&
+                           cn >= (need_node ? inst * (unsigned long long)d.nn : 0ull);
+        if (!ready) {
+          for (int o = 0; o < 3 && ok; o++) ok = wait_band(P, d, bands[o], inst);
+          if (ok && need_node)
+            ok = wait_done(P, P.ndone + item.dom, inst * (unsigned long long)d.nn);
+        }
       }
+      fence_acquire();
     }
-    // a wait that ran out stops every lane (the launch is aborted)
-    if (!__all_sync(0xffffffffu, ok)) break;
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    // a wait that ran out stops the warp (the launch is aborted)
+    if (!ok) break;
     if (item.type == PI_STRIP) {
       const StageArgs a = persist_stage_args(P, d, step, item.stage);
       const int c0 = BC + (item.index % d.sx) * SW;
@@ -837,11 +842,10 @@ __global__ void __launch_bounds__(32 * PW, 8) k_batch_persistent(const __grid_co
     } else {
       node_bc_cell(persist_node_args(P, d, step, item.stage), item.index * 32 + lane);
     }
-    // release: every lane's stores are performed device-wide (its fence),
-    // the warp barrier orders them before lane 0, whose fence (cumulative)
-    // precedes the counter increment.  The counter's address is looked up
-    // again from the item table rather than kept live across the work.
-    __threadfence();
+    // release: the warp barrier orders every lane's stores before lane 0,
+    // whose fence (cumulative) precedes the counter increment.  The
+    // counter's address is looked up again from the item table rather than
+    // kept live across the work.
     __syncwarp();
     if (lane == 0 && (long long)it != P.withhold) {
       __threadfence();
