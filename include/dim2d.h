@@ -317,10 +317,13 @@ DIM2D_API int dim2d_batch_set_graphs(dim2d_batch *b, int enable);
  * persistent kernel per precision (FP64, DIM2D_MIXED) that advances every
  * member by n steps.  Its warps take work items from one queue -- per step
  * and stage, the ghost cells of open sections and the strips of every
- * member, then the node boundary passes -- and an item starts once every
- * earlier item of its own field has completed, so fields of every boundary
- * kind and size advance together without grid-wide barriers.  Results are
- * those of the graph mode bit for bit (the same per-cell code).  Each wait
+ * member, then the node boundary passes -- and an item starts once the
+ * items of its field that it depends on have completed (the previous stage
+ * on its row band and the two next to it, the previous node pass), so fields
+ * of every boundary kind and size advance together without grid-wide
+ * barriers.  The per-cell code is the graph mode's; results agree with it to
+ * rounding (the compiler may contract the two instantiations differently).
+ * Each wait
  * is bounded (dim2d_batch_set_wait_limit, default 2 s); one that runs out
  * stops the launch and dim2d_batch_sync returns DIM2D_ERR_TIMEOUT. */
 DIM2D_API int dim2d_batch_set_persistent(dim2d_batch *b, int enable);
