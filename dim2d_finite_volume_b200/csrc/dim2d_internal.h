@@ -67,7 +67,8 @@ struct dim2d_handle {
   double* td = nullptr;  // time_dev buffer, allocated on first use
   double* x_map = nullptr;
   double* y_map = nullptr;
-  double* scalar = nullptr;  // reductions / status words
+  double* scalar = nullptr;  // [0] CFL reduction, [2] wall status word (status),
+                             // [3] health word of a served request (health_word)
   double dx = 0, dy = 0, rdx = 0, rdy = 0;
   double x_min = 0, x_max = 0, y_min = 0, y_max = 0;
   double t = 0;
@@ -142,6 +143,11 @@ int persist_steps(dim2d_handle* h, double dt, int nsteps, double dt_scale);
 cudaError_t launch_stage_work(dim2d_handle* h, const dim2d::StageArgs& a, int mode);
 int apply_bc_on_nodes(dim2d_handle* h, const double* nodes_tmp, double* nodes);
 int check_status(dim2d_handle* h);
+// device word the serving loop's check sets: bit 0 a non-finite value in the
+// field, bit 1 the wall status word set (zero at creation)
+inline unsigned int* health_word(dim2d_handle* h) {
+  return reinterpret_cast<unsigned int*>(h->scalar + 3);
+}
 // bracket one launch with profiling events (no-op unless h->prof)
 void prof_begin(dim2d_handle* h);
 void prof_end(dim2d_handle* h);

@@ -13,6 +13,12 @@
 //      steps; requests that reach their step count get their result copied
 //      to host memory right behind that chunk (same stream) and leave the
 //      batch before the next chunk is built.
+//   4. check: behind every chunk, one small kernel per member sets the
+//      member's health word if its state holds a non-finite value or its
+//      wall root failed (where the reference stops); the word travels to
+//      pinned host memory behind the chunk, and a flagged request leaves
+//      the batch at the next chunk boundary with the state it has, instead
+//      of being stepped to its last step.
 // So requests that arrive while others run are admitted as memory frees
 // up and advance in the same batched launches (continuous batching), and
 // the GPU always has the next chunk queued while the host admits/retires.
@@ -48,6 +54,7 @@ struct Request {
   double* result = nullptr;  // pinned: final state (4 nx ny) + wall status word
   size_t result_cap = 0;
   unsigned int status = 0;
+  unsigned int stopped = 0;  // health flags of a request that left early (or finished flagged)
   double t_final = 0;
   cudaEvent_t copied = nullptr;
   Clock::time_point t_submit, t_done;
@@ -79,6 +86,44 @@ struct dim2d_server {
 };
 
 namespace {
+
+// health word of a field: bit 0 if any value of its interior cells (4
+// planes) is not finite, bit 1 if its wall root status word is set.  Words
+// are only ever set (the conditions are terminal), so no reset is needed
+// between chunks.  (A ghost cell that blows up reaches the interior within
+// a step or two; the ghost cells of some presets are not all defined.)
+__global__ void k_health(const double* __restrict__ u, Field f, const unsigned int* status,
+                         unsigned int* out) {
+  bool bad = false;
+  const size_t nxi = (size_t)(f.nx - 2 * BC);
+  const size_t per_plane = (size_t)(f.ny - 2 * BC) * nxi;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < 4 * per_plane;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t v = i / per_plane, r = i % per_plane;
+    const size_t y = BC + r / nxi, x = BC + r % nxi;
+    bad |= !isfinite(u[v * f.plane + y * f.pitch + x]);
+  }
+  bad = __syncthreads_or(bad);
+  if (threadIdx.x == 0) {
+    unsigned int w = bad ? 1u : 0u;
+    if (blockIdx.x == 0 && status && *status) w |= 2u;
+    if (w) atomicOr(out, w);
+  }
+}
+
+cudaError_t launch_health(dim2d_handle* h, cudaStream_t s) {
+  const size_t n = 4 * (size_t)(h->f.ny - 2 * BC) * (h->f.nx - 2 * BC);
+  const unsigned blocks = (unsigned)std::min<size_t>(592, (n + 255) / 256);
+  k_health<<<blocks, 256, 0, s>>>(h->A, h->f, h->south_wall ? h->status : nullptr,
+                                  health_word(h));
+  return cudaGetLastError();
+}
+
+// pinned host copy of a request's health word: the slot after the status
+// word behind the result state
+unsigned int* health_host(Request* r) {
+  return reinterpret_cast<unsigned int*>(r->result + 4 * (size_t)r->nx * r->ny + 1);
+}
 
 cudaEvent_t get_event(dim2d_server* s) {
   if (!s->free_events.empty()) {
@@ -150,6 +195,7 @@ int retire(dim2d_server* s, int* completed) {
     r->t_done = Clock::now();
     r->state = R_DONE;
     std::memcpy(&r->status, r->result + 4 * (size_t)r->nx * r->ny, sizeof r->status);
+    r->stopped |= *health_host(r);
     s->free_events.push_back(r->copied);
     r->copied = nullptr;
     release(s, r);
@@ -188,15 +234,61 @@ int admit(dim2d_server* s) {
   return DIM2D_OK;
 }
 
+// final state -> pinned host memory, right behind the work queued so far;
+// the request leaves the batch
+int finish(dim2d_server* s, Request* r) {
+  const Field& f = r->h->f;
+  cudaError_t e = cudaMemcpy2DAsync(r->result, f.nx * sizeof(double), r->h->A, f.pitch * sizeof(double),
+                                    f.nx * sizeof(double), 4 * (size_t)f.ny,
+                                    cudaMemcpyDeviceToHost, s->stream);
+  unsigned int* st = reinterpret_cast<unsigned int*>(r->result + 4 * (size_t)f.nx * f.ny);
+  *st = 0;
+  if (e == cudaSuccess && r->h->south_wall)  // wall root status word, behind the state
+    e = cudaMemcpyAsync(st, r->h->status, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                        s->stream);
+  r->copied = get_event(s);
+  if (e == cudaSuccess) e = cudaEventRecord(r->copied, s->stream);
+  if (e != cudaSuccess) return cuda_error(e, "server result copy");
+  r->t_final = r->h->t;
+  const int rc = dim2d_batch_remove(s->batch, r->h);
+  if (rc) return rc;
+  r->state = R_COPYING;
+  s->copying.push_back(r);
+  return DIM2D_OK;
+}
+
 int run_chunk(dim2d_server* s) {
+  // requests an earlier chunk's check flagged leave now, with the state
+  // they have (the words read here may be a chunk old: flags only get set)
+  for (size_t i = 0; i < s->active.size();) {
+    Request* r = s->active[i];
+    const unsigned int flags = *(volatile unsigned int*)health_host(r);
+    if (!flags) {
+      i++;
+      continue;
+    }
+    r->stopped = flags;
+    const int rc = finish(s, r);
+    if (rc) return rc;
+    s->active.erase(s->active.begin() + i);
+  }
   if (s->active.empty()) return DIM2D_OK;
   long long k = s->chunk_steps;
   for (Request* r : s->active) k = std::min(k, r->remaining);
   int rc = dim2d_batch_step(s->batch, (int)k);
   if (rc) return rc;
+  // health checks of every member behind the chunk, their words to the host
+  cudaError_t e = cudaSuccess;
+  for (Request* r : s->active) {
+    e = launch_health(r->h, s->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(health_host(r), health_word(r->h), sizeof(unsigned int),
+                          cudaMemcpyDeviceToHost, s->stream);
+    if (e != cudaSuccess) return cuda_error(e, "server health check");
+  }
   Chunk c;
   c.done = get_event(s);
-  cudaError_t e = cudaEventRecord(c.done, s->stream);
+  e = cudaEventRecord(c.done, s->stream);
   if (e != cudaSuccess) return cuda_error(e, "server chunk");
   s->inflight.push_back(c);
   for (size_t i = 0; i < s->active.size();) {
@@ -207,24 +299,8 @@ int run_chunk(dim2d_server* s) {
       i++;
       continue;
     }
-    // final state -> pinned host memory, right behind the chunk
-    const Field& f = r->h->f;
-    e = cudaMemcpy2DAsync(r->result, f.nx * sizeof(double), r->h->A, f.pitch * sizeof(double),
-                          f.nx * sizeof(double), 4 * (size_t)f.ny, cudaMemcpyDeviceToHost,
-                          s->stream);
-    unsigned int* st = reinterpret_cast<unsigned int*>(r->result + 4 * (size_t)f.nx * f.ny);
-    *st = 0;
-    if (e == cudaSuccess && r->h->south_wall)  // wall root status word, behind the state
-      e = cudaMemcpyAsync(st, r->h->status, sizeof(unsigned int), cudaMemcpyDeviceToHost,
-                          s->stream);
-    r->copied = get_event(s);
-    if (e == cudaSuccess) e = cudaEventRecord(r->copied, s->stream);
-    if (e != cudaSuccess) return cuda_error(e, "server result copy");
-    r->t_final = r->h->t;
-    rc = dim2d_batch_remove(s->batch, r->h);
+    rc = finish(s, r);
     if (rc) return rc;
-    r->state = R_COPYING;
-    s->copying.push_back(r);
     s->active.erase(s->active.begin() + i);
   }
   return DIM2D_OK;
@@ -309,6 +385,7 @@ int dim2d_server_submit(dim2d_server* s, int nx, int ny, const int bc_choice[8],
     delete r;
     return set_error(DIM2D_ERR_NOMEM, "server_submit: pinned host buffers");
   }
+  *health_host(r) = 0;
   std::memcpy(r->staging, nodes, n * sizeof(double));
   std::memcpy(r->staging + n, x_map, nx * sizeof(double));
   std::memcpy(r->staging + n + nx, y_map, ny * sizeof(double));
@@ -350,13 +427,17 @@ int dim2d_server_result(dim2d_server* s, long long id, double* nodes, double* t,
   if (nodes) std::memcpy(nodes, r->result, 4 * (size_t)r->nx * r->ny * sizeof(double));
   if (t) *t = r->t_final;
   if (latency_s) *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
-  const unsigned int status = r->status;
+  const unsigned int status = r->status, stopped = r->stopped;
+  const long long done = r->nsteps - r->remaining;
   pinned_put(s, r->result, r->result_cap);
   s->all.erase(it);
   delete r;
   if (status)  // the reference stops where a wall ghost root fails
     return set_error(DIM2D_ERR_WALL_ROOT, "request %lld: wall ghost cell root (status 0x%x)",
                      id, status);
+  if (stopped & 1u)
+    return set_error(DIM2D_ERR_NONFINITE,
+                     "request %lld: state not finite (stopped after %lld steps)", id, done);
   return DIM2D_OK;
 }
 

@@ -33,7 +33,8 @@ FP64, MIXED = 0, 1
 
 ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "unsupported configuration",
           4: "device allocation refused", 5: "wall root not bracketed/converged",
-          6: "device wait timed out", 7: "state not uploaded"}
+          6: "device wait timed out", 7: "state not uploaded",
+          8: "state not finite"}
 
 
 class Dim2dError(RuntimeError):

@@ -46,6 +46,7 @@ def _lib():
 
 NOT_READY = 7
 WALL_ROOT = 5
+NONFINITE = 8
 STATS = ("pending", "active", "copying", "completed", "cell_updates", "bytes_in_use",
          "budget_bytes", "max_active")
 
@@ -83,9 +84,11 @@ class Server:
 
     def result(self, rid):
         """(nodes, time, latency_s, status), or None while the request runs.
-        status 0, or WALL_ROOT when a wall ghost-cell root failed during the
-        solve -- where the reference stops; nodes then hold the state the
-        solve ended with."""
+        status 0; WALL_ROOT when a wall ghost-cell root failed during the
+        solve -- where the reference stops; NONFINITE when the state stopped
+        being finite.  The server stops such requests at the chunk boundary
+        after its check saw them; nodes and time are then the state and time
+        the solve ended with."""
         out = np.empty(self.shapes.get(rid, (4, 1, 1)))  # unknown ids: the library errors
         t = ctypes.c_double()
         lat = ctypes.c_double()
@@ -94,7 +97,7 @@ class Server:
                                         ctypes.byref(lat))
         if rc == NOT_READY:
             return None
-        if rc != WALL_ROOT:
+        if rc not in (WALL_ROOT, NONFINITE):
             _check(rc)
         del self.shapes[rid]
         return out, t.value, lat.value, rc
@@ -127,13 +130,14 @@ def serve(server, requests, keep_results=False):
     nsteps, bc and optionally precision) in real time: each is submitted at
     its arrival time, the loop polls in between.  Returns dict(latencies, results (index ->
     (nodes, time) if keep_results), failed (indices of requests whose wall
-    root failed), nonfinite (other requests whose final state is not
-    finite), finished (the other requests: finite solves), wall_s,
-    cell_updates (all requests), cell_updates_finished (finished requests
-    only), stats)."""
+    root failed), nonfinite (other requests whose state stopped being
+    finite), finished (the other requests: finite solves), end_time (index
+    -> the time each solve ended at; earlier than dt * nsteps for requests
+    the server stopped), wall_s, cell_updates (all requests, as
+    requested), cell_updates_finished (finished requests only), stats)."""
     order = sorted(range(len(requests)), key=lambda i: requests[i]["arrival"])
     ids = {}
-    out, lat, failed, nonfinite = {}, {}, [], []
+    out, lat, failed, nonfinite, end_time = {}, {}, [], [], {}
     t0 = time.perf_counter()
     nxt = 0
     while len(lat) < len(requests):
@@ -154,9 +158,10 @@ def serve(server, requests, keep_results=False):
                 continue
             i = ids.pop(rid)
             lat[i] = res[2]
-            if res[3]:
+            end_time[i] = res[1]
+            if res[3] == WALL_ROOT:
                 failed.append(i)
-            elif not np.isfinite(res[0]).all():
+            elif res[3] == NONFINITE or not np.isfinite(res[0]).all():
                 nonfinite.append(i)
             if keep_results:
                 out[i] = (res[0], res[1])
@@ -166,7 +171,8 @@ def serve(server, requests, keep_results=False):
 
     bad = set(failed) | set(nonfinite)
     return dict(latencies=[lat[i] for i in range(len(requests))], results=out,
-                failed=sorted(failed), nonfinite=sorted(nonfinite), wall_s=wall,
+                failed=sorted(failed), nonfinite=sorted(nonfinite), end_time=end_time,
+                wall_s=wall,
                 cell_updates=sum(cells(r) for r in requests),
                 finished=[i for i in range(len(requests)) if i not in bad],
                 cell_updates_finished=sum(cells(r) for i, r in enumerate(requests)

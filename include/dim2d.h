@@ -49,6 +49,7 @@ extern "C" {
 #define DIM2D_ERR_WALL_ROOT 5    /* wall ghost-cell root not bracketed / not converged */
 #define DIM2D_ERR_TIMEOUT 6      /* a bounded device wait expired */
 #define DIM2D_ERR_NOT_READY 7    /* state not uploaded yet */
+#define DIM2D_ERR_NONFINITE 8    /* a served request's state is no longer finite */
 
 /* boundary choices: src/parameters/parameters_constant.f:145-152 */
 #define DIM2D_PERIODIC_X 0
@@ -360,7 +361,11 @@ DIM2D_API int dim2d_batch_destroy(dim2d_batch *b);
  * the device's stream-ordered pool; results land in pinned host memory.
  * dim2d_server_poll drives the loop (wait != 0: block until the oldest
  * queued chunk has finished); call it repeatedly.  Requests are FP64 or
- * DIM2D_MIXED, each in its own precision. */
+ * DIM2D_MIXED, each in its own precision.  Behind every chunk the server
+ * checks each member: a request whose interior state is no longer finite,
+ * or whose wall ghost-cell root failed, leaves at the next chunk boundary
+ * (one or two chunks later) with the state and time it has, instead of
+ * being stepped to its last step. */
 typedef struct dim2d_server dim2d_server;
 /* mem_budget: bytes of device memory for fields (0 = free memory less a
  * reserve; larger values are capped the same way) */
@@ -375,8 +380,10 @@ DIM2D_API int dim2d_server_submit(dim2d_server *s, int nx, int ny, const int bc_
 DIM2D_API int dim2d_server_poll(dim2d_server *s, int wait, int *completed);
 /* DIM2D_ERR_NOT_READY until the request is complete; then copies its final
  * nodes(nx,ny,4) and time, its latency (submit to completion, seconds),
- * and forgets the request.  DIM2D_ERR_WALL_ROOT (nodes still copied) if a
- * wall ghost-cell root failed during the solve. */
+ * and forgets the request.  DIM2D_ERR_WALL_ROOT (nodes and time still
+ * copied) if a wall ghost-cell root failed during the solve, else
+ * DIM2D_ERR_NONFINITE (likewise) if the state stopped being finite; the
+ * time then says how far the solve got. */
 DIM2D_API int dim2d_server_result(dim2d_server *s, long long id, double *nodes, double *t,
                                   double *latency_s);
 /* out[8]: pending, active, copying, completed, cell-updates issued, bytes

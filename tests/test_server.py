@@ -128,3 +128,32 @@ def test_result_protocol(F, S):
             big = np.zeros((4, 600, 600))
             S.Server(params=_params(), mem_budget=1 << 20).submit(big, np.linspace(0, 1, 600),
                                                 np.linspace(0, 1, 600), 1e-6, 10)
+
+
+def test_diverged_request_stops_early(F, S):
+    """A request whose state is not finite (a NaN planted in one interior
+    cell of an open field's initial state) is stopped at a chunk boundary
+    soon after the server's check sees it -- not stepped to its 4000th
+    step -- and reported as NONFINITE with the time it reached; the request
+    beside it ends as it does when served without the diverged one (same
+    batched kernel and shape: <= 1e-14 normwise, rounding of the contraction
+    at most)."""
+    reqs = _requests(2, seed=8, kinds=("hedstrom_xy",))
+    bad = dict(reqs[1])
+    bad["nodes"] = reqs[1]["nodes"].copy()
+    bad["nodes"][0, bad["ny"] // 2, bad["nx"] // 2] = np.nan
+    bad["nsteps"] = 4000
+    chunk = 16
+    with S.Server(params=_params(), chunk_steps=chunk) as srv:
+        run = S.serve(srv, [reqs[0], bad], keep_results=True)
+    assert run["nonfinite"] == [1] and run["failed"] == []
+    # flagged after the first chunk, seen by the host at most two chunks
+    # later (two chunks stay queued), stopped at the next boundary
+    assert run["end_time"][1] <= 4 * chunk * bad["dt"] * (1 + 1e-12), run["end_time"][1]
+    with S.Server(params=_params(), chunk_steps=chunk) as srv:
+        solo = S.serve(srv, [reqs[0]], keep_results=True)
+    got, t = run["results"][0]
+    ref, t_ref = solo["results"][0]
+    assert np.isfinite(got).all()
+    assert np.all(_err(got, ref, reqs[0]["bc"]) <= 1e-14)
+    assert abs(t - t_ref) <= 1e-12 * t_ref
