@@ -363,10 +363,19 @@ int dim2d_upload(dim2d_handle* h, const double* nodes, const double* x_map, cons
   if (!h || !nodes || !x_map || !y_map) return set_error(DIM2D_ERR_ARG, "upload: null argument");
   const Field& f = h->f;
   cudaError_t e = wait_copy_if(h, h->A);  // a pending asynchronous copy of A lands first
+  if (e == cudaSuccess) e = wait_copy_if(h, h->B);  // ... or of a stage buffer
+  if (e == cudaSuccess) e = wait_copy_if(h, h->C);
   if (e == cudaSuccess)
     e = cudaMemcpy2DAsync(h->A, f.pitch * sizeof(double), nodes, f.nx * sizeof(double),
                                     f.nx * sizeof(double), 4 * (size_t)f.ny,
                                     cudaMemcpyHostToDevice, h->stream);
+  // Ghost cells that no boundary operator writes (for a south wall: the
+  // energy of both ghost rows and the momenta of the outer one) keep the
+  // uploaded values in all three buffers, so the state holds them whichever
+  // buffer it is in.  (The reference adds dt times an unset time derivative
+  // there, compute_1st_step over all nodes, rk3tvd_steps_module.f:52-100,
+  // and never reads them.)
+  if (e == cudaSuccess) e = launch_copy_frame(h->A, h->B, h->C, f, h->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(h->x_map, x_map, f.nx * sizeof(double), cudaMemcpyHostToDevice,
                         h->stream);

@@ -139,6 +139,9 @@ cudaError_t launch_strip_masked(const StageArgs& a, cudaStream_t s);
 cudaError_t launch_open_ghosts(const StageArgs& a, int mode, cudaStream_t s);
 cudaError_t launch_fill(double* p, double v, size_t n, cudaStream_t s);
 cudaError_t launch_periodic_ghosts(double* u, const Field& f, cudaStream_t s);
+// the ghost frame (every cell within BC of an edge, 4 planes) of src into d1 and d2
+cudaError_t launch_copy_frame(const double* src, double* d1, double* d2, const Field& f,
+                              cudaStream_t s);
 cudaError_t launch_cfl_max(const double* u, const Field& f, const DimConst& k, double* out,
                            cudaStream_t s);
 

@@ -161,6 +161,35 @@ def test_persistent_long_run_matches_graph_mode(F, B, rows):
         assert np.all(err <= 1e-9), (d["bc"], d["nx"], err)
 
 
+WALL_PRESETS = ("wall_S_reflection", "half_wall_S_open", "wall_S_open")
+
+
+def test_unwritten_ghost_cells_keep_uploaded_values(F, B, cases):
+    """Ghost cells that no boundary operator writes -- on a south wall the
+    energy of both ghost rows and the momenta of the outer one (the wall
+    pass sets the density ghosts and the inner momenta) -- keep the uploaded
+    values whichever of the ping-pong buffers holds the state: after an odd
+    number of steps, alone, in the graph mode and in the persistent mode;
+    and the two batch modes then agree over all cells, ghosts included."""
+    walls = [c for c in cases if c[0] in WALL_PRESETS]
+    graph = _run(F, B, walls, (7,), persistent=False)
+    pers = _run(F, B, walls, (7,), persistent=True)
+    for (p, nx, ny, x_map, y_map, q, dt), (g, _), (r, _) in zip(walls, graph, pers):
+        assert np.all(normwise_rel_err_all(r, g) <= 1e-13), (p, normwise_rel_err_all(r, g))
+        for out in (g, r):
+            assert np.array_equal(out[3, :2, 2:-2], q[3, :2, 2:-2]), p  # energy, both rows
+            assert np.array_equal(out[1:3, 0, 2:-2], q[1:3, 0, 2:-2]), p  # momenta, outer row
+    p, nx, ny, x_map, y_map, q, dt = walls[0]
+    with F.Field(nx, ny, bc=p) as fld:
+        fld.ini(q, x_map, y_map)
+        fld.apply_bc_on_nodes()  # field%ini
+        fld.variant = 2
+        fld.integrate(dt, 7)
+        out = fld.download()
+    assert np.array_equal(out[3, :2, 2:-2], q[3, :2, 2:-2])
+    assert np.array_equal(out[1:3, 0, 2:-2], q[1:3, 0, 2:-2])
+
+
 def test_persistent_autotune_keeps_state(F, B, cases):
     (out, chosen, times) = _run(F, B, cases[:4], (3,), persistent=True, autotune=True)
     assert all(c in (8, 16, 32) for c in chosen)
