@@ -157,3 +157,20 @@ def test_diverged_request_stops_early(F, S):
     assert np.isfinite(got).all()
     assert np.all(_err(got, ref, reqs[0]["bc"]) <= 1e-14)
     assert abs(t - t_ref) <= 1e-12 * t_ref
+
+
+def test_wall_root_failure_stops_early(F, S):
+    """A 64^2 wall bubble with a 4-dx interface under the test constants
+    (We = 10) collapses and its wall ghost-cell root stops being bracketed
+    after about 136 steps (the oracle fails at that step, where the reference
+    stops); the server's check sees the wall status word and stops the
+    request at a chunk boundary shortly after, with DIM2D_ERR_WALL_ROOT,
+    instead of stepping it to its 4000th step."""
+    from dim2d_finite_volume_b200 import workloads
+    d = workloads.domain(64, T0=0.95, bubbles=[(0.0, 0.0, 0.2)], bc="wall_S_reflection")
+    req = dict(d, arrival=0.0, nsteps=4000, precision=0)
+    with S.Server(params=F.default_params(), chunk_steps=16) as srv:
+        run = S.serve(srv, [req])
+    assert run["failed"] == [0], run
+    steps = run["end_time"][0] / d["dt"]
+    assert 100 <= steps <= 400, steps  # failure near step 136, then at most a few chunks
