@@ -258,7 +258,11 @@ enum NodeF : int {
 };
 constexpr int NM = 3;              // node rows (y-1 .. y+1)
 constexpr int F_ROW = NQF * PC;    // floats per node row
-constexpr int WARP_DOUBLES_MIX = NS * ST_ROW + NM * PC + (NM * F_ROW + 1) / 2 + 2 * UN_ROW;
+// Mixed precision keeps one u^n row (FP64 keeps two, alternating): the next
+// row's u^n is copied once the update has read this one, in its own
+// cp.async group, and waited for just before the next update.  10.8 KB per
+// warp then fits 20 warps per SM (shape 16x4x5, 96 registers).
+constexpr int WARP_DOUBLES_MIX = NS * ST_ROW + NM * PC + (NM * F_ROW + 1) / 2 + UN_ROW;
 #define FQ(o, c, dc) reinterpret_cast<float*>(g_ring)[(o) + (c) * PC + (dc)]
 #define KQ(o, dc) g_ring[(o) + (dc)]
 
@@ -431,7 +435,7 @@ __device__ __forceinline__ void strip_warp(const StageArgs& a, int c0, int y0, i
   // u^n rows (two, alternating), after the rest of the warp's region
   const int unb = wbase + (MIX ? NS * ST_ROW + NM * PC + (NM * F_ROW + 1) / 2
                                : NS * ST_ROW + NUV * UV_ROW + NQ * Q_ROW) + lane;
-  int un0 = unb, un1 = unb + UN_ROW;
+  int un0 = unb, un1 = MIX ? unb : unb + UN_ROW;
 
   if (a.node_sides && reads_node_ghosts(a.node_sides, f, c0, y0, y1)) wait_for_node_pass();
 
@@ -459,6 +463,7 @@ __device__ __forceinline__ void strip_warp(const StageArgs& a, int c0, int y0, i
   else y_face<WALL>(a, s2, s0, um, u0, q1, q0, x, y0 - 1, Gb);
   __syncwarp();  // rows y0-2 and y0-1 are no longer read
   async_row(a, c0, y0 + 2, lane, s2);
+  if (MIX) cp_async_commit();  // mixed: u^n rows travel in their own groups
   if (need_un) async_un(a, c0, y0, un0, lane);
   cp_async_commit();
 
@@ -477,9 +482,12 @@ __device__ __forceinline__ void strip_warp(const StageArgs& a, int c0, int y0, i
 #pragma unroll 1
   for (int y = y0; y < y1; y++) {
     async_row(a, c0, y + 3, lane, s3);  // next row: lands during this one
-    if (need_un) async_un(a, c0, y + 1, un1, lane);
+    if (!MIX && need_un) async_un(a, c0, y + 1, un1, lane);
     cp_async_commit();
-    cp_async_wait<1>();  // all but the group just issued: rows y+2, u^n(y)
+    // FP64: all but the group just issued (rows y+2, u^n(y)); mixed: all
+    // but that one and u^n(y)'s, which is waited for before the update
+    if (MIX) cp_async_wait<2>();
+    else cp_async_wait<1>();
     __syncwarp();
     if (MIX) node_row_mix(s0, s1, s2, f1, k1, qrdx, qrdy, hrdx2, hrdy2, k);
     else node_row(s0, s1, s2, u1, q1, qrdx, qrdy, hrdx2, hrdy2, k);
@@ -495,6 +503,10 @@ __device__ __forceinline__ void strip_warp(const StageArgs& a, int c0, int y0, i
     double Fr[4];
 #pragma unroll
     for (int v = 0; v < 4; v++) Fr[v] = __shfl_down_sync(0xffffffffu, Fx[v], 1);
+    if (MIX) {
+      cp_async_wait<1>();  // u^n(y)
+      __syncwarp();
+    }
     {
       // every lane evaluates the update; only active lanes store
       const size_t go = (size_t)y * f.pitch + min(x, f.nx - 1 - BC);
@@ -535,6 +547,10 @@ __device__ __forceinline__ void strip_warp(const StageArgs& a, int c0, int y0, i
 #pragma unroll
     for (int v = 0; v < 4; v++) Gb[v] = Gt[v];
     __syncwarp();  // row y and u^n(y) are no longer read
+    if (MIX) {  // mixed: one u^n slot, refilled now that row y is done
+      if (need_un) async_un(a, c0, y + 1, un0, lane);
+      cp_async_commit();
+    }
     const int t = s0;
     s0 = s1;
     s1 = s2;
