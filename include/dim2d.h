@@ -205,7 +205,9 @@ DIM2D_API int dim2d_profile_read(dim2d_handle *h, double *ms, long long *launche
 /* No counterpart in the reference (its stage loops have one fixed shape).
  * Stage-kernel variant: 0 = 32x8-cell CTA tiles; 1..5 = warp-streaming
  * strips 30 columns wide with (rows per warp, warps per CTA, resident CTAs
- * per SM) = (8,4,4), (16,4,4), (16,4,5), (16,2,8), (16,8,2); 6 = the
+ * per SM) = (8,4,4), (16,4,4), (16,4,5), (16,2,8), (16,8,2) (FP64 fields
+ * fit 16 warps per SM whatever the request; DIM2D_MIXED fields on (16,4,5)
+ * run 20); 6 = the
  * persistent kernel of batches (dim2d_batch_set_persistent) over this field
  * alone: each dim2d_step call is one launch whose warps take 16-row strips
  * stage by stage, a band starting its next stage as soon as it and its
