@@ -362,22 +362,9 @@ cudaError_t launch_fill(double* p, double v, size_t n, cudaStream_t s) {
 // into d1 and d2
 __global__ void k_copy_frame(const double* __restrict__ src, double* __restrict__ d1,
                              double* __restrict__ d2, Field f) {
-  const int rows = 2 * BC * f.nx;                  // BC rows at the bottom and at the top
-  const int per_plane = rows + (f.ny - 2 * BC) * 2 * BC;  // + BC columns on each side
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= 4 * per_plane) return;
-  const int v = i / per_plane, j = i % per_plane;
-  int x, y;
-  if (j < rows) {
-    const int r = j / f.nx;
-    x = j % f.nx;
-    y = r < BC ? r : f.ny - 2 * BC + r;
-  } else {
-    const int c = (j - rows) % (2 * BC);
-    y = BC + (j - rows) / (2 * BC);
-    x = c < BC ? c : f.nx - 2 * BC + c;
-  }
-  const size_t o = (size_t)v * f.plane + (size_t)y * f.pitch + x;
+  if (i >= frame_cells(f)) return;
+  const size_t o = frame_offset(f, i);
   const double q = src[o];
   d1[o] = q;
   d2[o] = q;
@@ -385,7 +372,7 @@ __global__ void k_copy_frame(const double* __restrict__ src, double* __restrict_
 
 cudaError_t launch_copy_frame(const double* src, double* d1, double* d2, const Field& f,
                               cudaStream_t s) {
-  const int n = 4 * (2 * BC * f.nx + (f.ny - 2 * BC) * 2 * BC);
+  const int n = frame_cells(f);
   k_copy_frame<<<(n + 255) / 256, 256, 0, s>>>(src, d1, d2, f);
   return cudaGetLastError();
 }

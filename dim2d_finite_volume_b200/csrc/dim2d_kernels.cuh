@@ -139,7 +139,30 @@ cudaError_t launch_strip_masked(const StageArgs& a, cudaStream_t s);
 cudaError_t launch_open_ghosts(const StageArgs& a, int mode, cudaStream_t s);
 cudaError_t launch_fill(double* p, double v, size_t n, cudaStream_t s);
 cudaError_t launch_periodic_ghosts(double* u, const Field& f, cudaStream_t s);
-// the ghost frame (every cell within BC of an edge, 4 planes) of src into d1 and d2
+// The ghost frame of a field: every cell within BC of an edge, 4 planes.
+// frame_cells counts them; frame_offset(f, i), 0 <= i < frame_cells(f), is
+// the offset of cell i in the planar layout (per plane: the BC bottom rows,
+// the BC top rows, then the BC left and BC right cells of each row between).
+inline __host__ __device__ int frame_cells(const Field& f) {
+  return 4 * (2 * BC * f.nx + (f.ny - 2 * BC) * 2 * BC);
+}
+inline __host__ __device__ size_t frame_offset(const Field& f, int i) {
+  const int rows = 2 * BC * f.nx;
+  const int per_plane = rows + (f.ny - 2 * BC) * 2 * BC;
+  const int v = i / per_plane, j = i % per_plane;
+  int x, y;
+  if (j < rows) {
+    const int r = j / f.nx;
+    x = j % f.nx;
+    y = r < BC ? r : f.ny - 2 * BC + r;
+  } else {
+    const int c = (j - rows) % (2 * BC);
+    y = BC + (j - rows) / (2 * BC);
+    x = c < BC ? c : f.nx - 2 * BC + c;
+  }
+  return (size_t)v * f.plane + (size_t)y * f.pitch + x;
+}
+// the ghost frame of src into d1 and d2
 cudaError_t launch_copy_frame(const double* src, double* d1, double* d2, const Field& f,
                               cudaStream_t s);
 cudaError_t launch_cfl_max(const double* u, const Field& f, const DimConst& k, double* out,
