@@ -113,6 +113,7 @@ __global__ void k_health(const double* __restrict__ u, Field f, const unsigned i
 
 cudaError_t launch_health(dim2d_handle* h, cudaStream_t s) {
   const size_t n = 4 * (size_t)(h->f.ny - 2 * BC) * (h->f.nx - 2 * BC);
+  // grid-stride: at most 4 CTAs of 256 threads per SM on a 148-SM B200
   const unsigned blocks = (unsigned)std::min<size_t>(592, (n + 255) / 256);
   k_health<<<blocks, 256, 0, s>>>(h->A, h->f, h->south_wall ? h->status : nullptr,
                                   health_word(h));
