@@ -1,8 +1,9 @@
 """GPU parity at the lengths and sizes of the benchmarked configurations,
 through the C ABI, against the oracle.
 
-* The plain FP64 configurations with the stage-kernel variant the bench
-  uses (4 = k_strip<16,2,8>) and the one the autotuner picks, 100 RK3 steps:
+* The plain FP64 configurations with stage-kernel variant 4 (k_strip<16,2,8>),
+  the one the autotuner picks and the persistent kernel (variant 6, the 100
+  steps as one launch), 100 RK3 steps:
   the 128^2 periodic bubble (132^2 nodes) and the 1024^2 open-boundary
   bubble of the headline workload (1028^2 nodes, whole field) -- bar 1e-10
   normwise, the north star's.
@@ -31,6 +32,7 @@ from tests.helpers import normwise_rel_err, normwise_rel_err_all, periodic_case,
 pytestmark = pytest.mark.gpu
 
 BENCH_VARIANT = 4
+PERSISTENT_VARIANT = 6  # the persistent kernel: all 100 steps in one launch
 BATCH_SEED = 1311  # the bench's batched workload (seed 1234 + 77)
 
 
@@ -79,7 +81,7 @@ def _run_field(F, bc, q, x_map, y_map, dt, nsteps, variant, params=None, precisi
         return fld.download(), variant
 
 
-@pytest.mark.parametrize("variant", [BENCH_VARIANT, "auto"])
+@pytest.mark.parametrize("variant", [BENCH_VARIANT, "auto", PERSISTENT_VARIANT])
 def test_periodic_128_100_steps(orc, F, variant):
     nx, ny, x_map, y_map, q = periodic_case(128)
     cfg = _cfg(orc, F, "periodic_xy", nx, ny)
@@ -106,7 +108,7 @@ def open_1024(orc, F):
     return w, ref
 
 
-@pytest.mark.parametrize("variant", [BENCH_VARIANT, "auto"])
+@pytest.mark.parametrize("variant", [BENCH_VARIANT, "auto", PERSISTENT_VARIANT])
 def test_open_1024_100_steps(open_1024, F, variant):
     w, ref = open_1024
     got, v = _run_field(F, "hedstrom_xy", w["nodes"], w["x_map"], w["y_map"], w["dt"], 100,
