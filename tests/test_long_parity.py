@@ -119,45 +119,58 @@ def test_open_1024_100_steps(open_1024, F, variant):
     assert np.all(err <= 1e-10), (v, err)
 
 
-@pytest.fixture(scope="module")
-def wall_1024(orc, F):
-    """The reference's default preset half_wall_S_open (S wall, W mirror, N
-    and E open; the test constants: no wall heat source, 90 degree contact
-    angle) on the headline field's bubble at rest, after field%ini's node
-    pass, and the oracle's state after 100 steps (whole 1028^2 field, all
-    host cores)."""
+WALL_PRESETS = ("half_wall_S_open", "wall_S_open", "wall_S_reflection", "reflection_xy")
+
+
+@pytest.fixture(scope="module", params=WALL_PRESETS)
+def wall_1024(request, orc, F):
+    """The presets with a node pass -- the reference's default
+    half_wall_S_open (S wall, W mirror, N and E open), wall_S_open,
+    wall_S_reflection and reflection_xy; the test constants: no wall heat
+    source, 90 degree contact angle -- on the headline field's bubble at
+    rest, after field%ini's node pass, and the oracle's state after 100 steps
+    (whole 1028^2 field, all host cores).  Returns (preset, workload, state)."""
     from dim2d_finite_volume_b200 import workloads
-    w = workloads.plain_1024(1234, 1024, "half_wall_S_open")
-    cfg = _cfg(orc, F, "half_wall_S_open", w["nx"], w["ny"])
+    preset = request.param
+    w = workloads.plain_1024(1234, 1024, preset)
+    cfg = _cfg(orc, F, preset, w["nx"], w["ny"])
     q = w["nodes"].copy()
     orc.lib().orc_clear_status()
     orc.apply_bc_on_nodes(cfg, 0.0, w["x_map"], w["y_map"], q.copy(), q)
     ref = q.copy()
     orc.integrate(cfg, ref, w["x_map"], w["y_map"], 0.0, w["dt"], 100)
-    return w, ref
+    return preset, w, ref
 
 
 @pytest.mark.parametrize("variant", [BENCH_VARIANT, "auto"])
-def test_half_wall_S_open_1024_100_steps(wall_1024, F, variant):
-    w, ref = wall_1024
-    got, v = _run_field(F, "half_wall_S_open", w["nodes"], w["x_map"], w["y_map"], w["dt"],
-                        100, variant)
-    err = _err(got, ref, "half_wall_S_open")
-    print("half_wall_S_open 1024^2, variant %s, 100 steps:" % v, err)
+def test_wall_presets_1024_100_steps(wall_1024, F, variant):
+    preset, w, ref = wall_1024
+    got, v = _run_field(F, preset, w["nodes"], w["x_map"], w["y_map"], w["dt"], 100, variant)
+    err = _err(got, ref, preset)
+    print("%s 1024^2, variant %s, 100 steps:" % (preset, v), err)
     assert np.isfinite(got[:, 2:-2, 2:-2]).all()
     assert np.all(err <= 1e-10), (v, err)
 
 
-@pytest.mark.parametrize("bc", ["hedstrom_xy", "half_wall_S_open"])
-def test_mixed_1024_100_steps(open_1024, wall_1024, F, bc):
-    """Mixed precision at the headline size against the FP64 oracle, on the
-    autotuned shape: the north star's 1e-5 bar."""
-    w, ref = open_1024 if bc == "hedstrom_xy" else wall_1024
+def _mixed_check(F, bc, w, ref):
     got, v = _run_field(F, bc, w["nodes"], w["x_map"], w["y_map"], w["dt"], 100, "auto",
                         precision=F.MIXED)
     err = _err(got, ref, bc)
     print("mixed %s 1024^2, variant %s, 100 steps:" % (bc, v), err)
     assert np.all(err <= 1e-5), (bc, v, err)
+
+
+def test_mixed_open_1024_100_steps(open_1024, F):
+    """Mixed precision at the headline size against the FP64 oracle, on the
+    autotuned shape: the north star's 1e-5 bar."""
+    w, ref = open_1024
+    _mixed_check(F, "hedstrom_xy", w, ref)
+
+
+def test_mixed_wall_presets_1024_100_steps(wall_1024, F):
+    """The same for every preset with a node pass."""
+    preset, w, ref = wall_1024
+    _mixed_check(F, preset, w, ref)
 
 
 def _batch_domains(indices):
